@@ -1,0 +1,255 @@
+// Device-side building blocks shared by every kernel of the depth peeler.
+//
+// Geometry is binary64 in the normalised image window [0,1]^2, exactly as in
+// the reference GPU route (warp_peel/kernels.py:9-21,139-250).  Bounding boxes
+// for the hierarchies are padded binary32 (kernels.py:235-250).  All code here
+// is compiled with -fmad=false, so every predicate is plain IEEE binary64 and a
+// CPU restatement of the same expression gives the same bits.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace edp {
+
+constexpr int kMaxVertices = 32;      // polygon register width (kernels.py:10)
+constexpr int kSourceVertices = 8;    // triangle + near plane + 4 window planes
+constexpr double kEps = 1.0e-10;      // cleanup scale in the unit window (kernels.py:11)
+constexpr float kPad = 2.0e-7f;       // binary32 box padding (kernels.py:244-249)
+constexpr int kCandidatesPerPass = 32;  // bounded traversal per thread (frontier.py:149)
+
+// Status slots (kernels.py:17-21, warp_peel/README.md:175-184).
+enum StatusSlot : int {
+  kResidual = 0, kNextResidual = 1, kPolygons = 2, kTriangles = 3, kLayers = 4,
+  kPass = 5, kBoundaryVertices = 6, kDepthTies = 8, kError = 9, kMaxHidden = 10,
+  kPeakResidual = 12, kStatusSlots = 16
+};
+// Error bits (kernels.py:20-21, warp_peel/EVENTS.md:203-207).
+enum ErrorBit : int {
+  kErrPolygon = 1, kErrWorker = 2, kErrResidual = 4, kErrOutput = 8, kErrVertices = 16,
+  kErrTriangles = 32, kErrLayers = 64, kErrEdgeNoding = 128, kErrInput = 256,
+  kErrHits = 1024, kErrRounds = 2048
+};
+// EventPeeler counters (warp_peel/events.py:816-844).
+enum Metric : int {
+  kTargetVisits = 0, kContourTests, kSplits, kRayGroups, kRayCandidateTests, kRayHits,
+  kRounds, kUniqueContours, kHeavyRayGroups, kBeamAttempts, kCertifiedBeams,
+  kBeamCandidateTests, kHeavyBeams, kRankComponents, kRankConnections,
+  kConnectionContourTests, kMergedPolygons, kMatchedPatchEdges, kEdgeHashMisses, kMetrics
+};
+
+// ---------------------------------------------------------------- vectors
+struct V2 { double x, y; };
+__host__ __device__ inline V2 v2(double x, double y) { return V2{x, y}; }
+__host__ __device__ inline V2 operator+(V2 a, V2 b) { return V2{a.x + b.x, a.y + b.y}; }
+__host__ __device__ inline V2 operator-(V2 a, V2 b) { return V2{a.x - b.x, a.y - b.y}; }
+__host__ __device__ inline V2 operator*(double s, V2 a) { return V2{s * a.x, s * a.y}; }
+__host__ __device__ inline V2 operator/(V2 a, double s) { return V2{a.x / s, a.y / s}; }
+__host__ __device__ inline bool operator==(V2 a, V2 b) { return a.x == b.x && a.y == b.y; }
+__host__ __device__ inline bool operator!=(V2 a, V2 b) { return !(a == b); }
+__host__ __device__ inline double dot(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
+__device__ inline double length(V2 a) { return sqrt(a.x * a.x + a.y * a.y); }
+// Lexicographic order of points (event_kernels.py:66-68).
+__host__ __device__ inline bool less(V2 a, V2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
+
+// Orientation of c relative to a->b: positive on the left (kernels.py:139-143).
+__host__ __device__ inline double cross(V2 a, V2 b, V2 c) {
+  V2 u = b - a, v = c - a;
+  return u.x * v.y - u.y * v.x;
+}
+
+// Affine depth plane s = (a, b, c): value a x + b y + c (kernels.py:179-181).
+struct Plane { double a, b, c, pad; };
+__host__ __device__ inline double value(const Plane &s, V2 x) { return s.a * x.x + s.b * x.y + s.c; }
+
+// ---------------------------------------------------------------- polygons
+// Remove near-duplicate points and collapse slivers (kernels.py:146-176):
+// points closer than EPS/100 merge, and a translation-stable area/perimeter
+// test drops polygons narrower than about EPS.  Returns the new size (0 when
+// the polygon collapsed); sizes above kMaxVertices are returned unchanged so
+// that the caller can raise the polygon-capacity error.
+__device__ inline int clean(V2 *p, int n) {
+  if (n > kMaxVertices) return n;
+  int count = 0;
+  const double merge = kEps * 0.01;
+  for (int j = 0; j < n; ++j) {
+    V2 x = p[j];
+    if (count == 0 || length(x - p[count - 1]) > merge) p[count++] = x;
+  }
+  if (count > 1 && length(p[0] - p[count - 1]) <= merge) --count;
+  if (count < 3) return 0;
+  V2 origin = p[0];
+  double area2 = 0.0, perimeter = 0.0;
+  for (int j = 0; j < count; ++j) {
+    V2 a = p[j], b = p[(j + 1) % count];
+    area2 += cross(origin, a, b);
+    perimeter += fabs(b.x - a.x) + fabs(b.y - a.y);
+  }
+  if (area2 <= kEps * perimeter) return 0;
+  return count;
+}
+
+__device__ inline int append(V2 *p, int n, V2 x) {
+  if (n < kMaxVertices) p[n] = x;
+  return n + 1;
+}
+
+// Split a convex polygon by the line s(x - anchor) = 0 into the part with
+// s >= 0 (inside) and s <= 0 (outside), then clean both (kernels.py:184-203).
+// Evaluating relative to the anchor keeps short clipping edges in place.
+__device__ inline void split_at(const V2 *p, int n, const Plane &s, V2 anchor, V2 *in, int &ni,
+                                V2 *out, int &no) {
+  ni = 0;
+  no = 0;
+  for (int j = 0; j < n; ++j) {
+    V2 a = p[j], b = p[(j + 1) % n];
+    double da = value(s, a - anchor), db = value(s, b - anchor);
+    if (da >= 0.0) ni = append(in, ni, a);
+    if (da <= 0.0) no = append(out, no, a);
+    if ((da > 0.0 && db < 0.0) || (da < 0.0 && db > 0.0)) {
+      V2 x = a + (da / (da - db)) * (b - a);
+      ni = append(in, ni, x);
+      no = append(out, no, x);
+    }
+  }
+  ni = clean(in, ni);
+  no = clean(out, no);
+}
+
+// Split by the supporting line of edge a->b: inside is to the left.
+__device__ inline void split_edge(const V2 *p, int n, V2 a, V2 b, V2 *in, int &ni, V2 *out,
+                                  int &no) {
+  V2 d = b - a;
+  Plane s{-d.y, d.x, 0.0, 0.0};
+  split_at(p, n, s, a, in, ni, out, no);
+}
+
+// Some edge of a has no vertex of b strictly on its left (kernels.py:219-232).
+__device__ inline bool separated(const V2 *a, int na, const V2 *b, int nb) {
+  for (int j = 0; j < na; ++j) {
+    bool positive = false;
+    for (int k = 0; k < nb; ++k)
+      if (cross(a[j], a[(j + 1) % na], b[k]) > 0.0) positive = true;
+    if (!positive) return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------- boxes
+struct Box { float4 lo, hi; };
+__device__ inline float4 empty_lo() { return make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f); }
+__device__ inline float4 empty_hi() { return make_float4(-1.0e30f, -1.0e30f, -1.0e30f, 0.f); }
+
+// Padded binary32 bounds of a polygon with depth (kernels.py:235-250).
+__device__ inline void polygon_bounds(const V2 *p, int n, const Plane &score, float4 &lo,
+                                      float4 &hi) {
+  double lx = 1.0e30, ly = 1.0e30, lz = 1.0e30, hx = -1.0e30, hy = -1.0e30, hz = -1.0e30;
+  for (int j = 0; j < n; ++j) {
+    double z = value(score, p[j]);
+    lx = fmin(lx, p[j].x); ly = fmin(ly, p[j].y); lz = fmin(lz, z);
+    hx = fmax(hx, p[j].x); hy = fmax(hy, p[j].y); hz = fmax(hz, z);
+  }
+  double pz = 2.0e-7 * fmax(1.0, fmax(fabs(lz), fabs(hz)));
+  lo = make_float4(float(lx - 2.0e-7), float(ly - 2.0e-7), float(lz - pz), 0.f);
+  hi = make_float4(float(hx + 2.0e-7), float(hy + 2.0e-7), float(hz + pz), 0.f);
+}
+
+// ---------------------------------------------------------------- hierarchy
+// A complete binary tree over a power-of-two number of Morton-ordered leaves,
+// one item per leaf; node 1 is the root, node i has children 2i and 2i+1 and
+// leaves are nodes [size, 2 size).  The size lives in device memory so one
+// captured graph serves any leaf count up to the allocated capacity
+// (solver.py:34-89, kernels.py:24-116).
+struct Tree {
+  const float4 *lo;
+  const float4 *hi;
+  const int *ids;
+  const int *size;  // device scalar: number of leaves (power of two)
+};
+
+__device__ inline int successor(int node) {
+  while (node > 0 && (node & 1) != 0) node >>= 1;
+  if (node > 0) node += 1;
+  return node;
+}
+
+__device__ inline bool overlaps(float4 a, float4 b, float4 lo, float4 hi) {
+  return a.x <= hi.x && a.y <= hi.y && a.z <= hi.z && b.x >= lo.x && b.y >= lo.y &&
+         b.z >= lo.z;
+}
+
+// Stackless depth-first step: advance from `node` to the next overlapping
+// leaf, stopping at `end` (0 for a whole-tree walk).  Returns the item id in
+// `found` (or -1) and the node at which to resume (kernels.py:41-64,
+// event_kernels.py:172-193).
+__device__ inline int query_next(const Tree &t, int leaves, float4 lo, float4 hi, int node,
+                                 int end, int &found) {
+  found = -1;
+  while (node > 0 && node != end) {
+    float4 a = __ldg(&t.lo[node]), b = __ldg(&t.hi[node]);
+    if (overlaps(a, b, lo, hi)) {
+      if (node < leaves) {
+        node = 2 * node;
+      } else {
+        found = __ldg(&t.ids[node - leaves]);
+        node = successor(node);
+        break;
+      }
+    } else {
+      node = successor(node);
+    }
+  }
+  return node;
+}
+
+// 15 bits per axis Morton code of a box centre clamped to [0,1] (kernels.py:67-91).
+__host__ __device__ inline uint32_t part1by1(uint32_t x) {
+  x &= 0x0000ffffu;
+  x = (x | (x << 8)) & 0x00ff00ffu;
+  x = (x | (x << 4)) & 0x0f0f0f0fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  return x;
+}
+
+// ---------------------------------------------------------------- hashing
+// SplitMix64 finaliser (Steele, Lea and Flood 2014), a public-domain mixer.
+__host__ __device__ inline uint64_t mix64(uint64_t x) {
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+// Bits of a double with -0 folded onto +0, so that equal values hash equally.
+__device__ inline uint64_t key_bits(double v) {
+  return v == 0.0 ? 0ull : static_cast<uint64_t>(__double_as_longlong(v));
+}
+
+// Order-preserving map of a double onto uint64 (for radix sorting).
+__device__ inline uint64_t ordered_bits(double v) {
+  uint64_t b = static_cast<uint64_t>(__double_as_longlong(v == 0.0 ? 0.0 : v));
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__device__ inline double atomic_min_double(double *addr, double v) {
+  unsigned long long *a = reinterpret_cast<unsigned long long *>(addr);
+  unsigned long long old = *a, assumed;
+  while (v < __longlong_as_double(old)) {
+    assumed = old;
+    old = atomicCAS(a, assumed, static_cast<unsigned long long>(__double_as_longlong(v)));
+    if (old == assumed) break;
+  }
+  return __longlong_as_double(old);
+}
+__device__ inline double atomic_max_double(double *addr, double v) {
+  unsigned long long *a = reinterpret_cast<unsigned long long *>(addr);
+  unsigned long long old = *a, assumed;
+  while (v > __longlong_as_double(old)) {
+    assumed = old;
+    old = atomicCAS(a, assumed, static_cast<unsigned long long>(__double_as_longlong(v)));
+    if (old == assumed) break;
+  }
+  return __longlong_as_double(old);
+}
+
+__device__ inline void set_error(int *status, int bit) { atomicOr(&status[kError], bit); }
+
+}  // namespace edp

@@ -1,0 +1,182 @@
+// Host-side declarations shared by the translation units of libedp_b200.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "edp_device.cuh"
+
+namespace edp {
+
+#define EDP_CHECK(call)                                  \
+  do {                                                   \
+    cudaError_t err__ = (call);                          \
+    if (err__ != cudaSuccess) return err__;              \
+  } while (0)
+
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortBlock * kSortItems;  // keys per radix tile
+constexpr int kScanTile = 2048;
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline int64_t pow2_at_least(int64_t v) {
+  int64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+inline unsigned grid_for(int64_t n, int block) {
+  int64_t g = ceil_div(n > 0 ? n : 1, block);
+  return static_cast<unsigned>(g);
+}
+
+// ---------------------------------------------------------------- primitives
+// Scratch for scans and radix sorts, sized once for the largest pool.
+struct SortScratch {
+  int *hist = nullptr;     // [256][tiles]
+  int *totals = nullptr;   // [256]
+  int *partials = nullptr; // scan tile sums
+  int64_t tiles = 0;       // capacity in radix tiles
+  int64_t scan_tiles = 0;  // capacity in scan tiles
+};
+
+// Exclusive scan of in[0, *count) into out; out[*count..capacity) untouched.
+// The total is written to *total.  Counts are read on the device.
+cudaError_t scan_exclusive(const int *in, int *out, const int *count, int64_t capacity,
+                           int *total, SortScratch &s, cudaStream_t st);
+
+// Stable LSD radix sort of (key, value) pairs over the first *count items
+// (device scalar); items at and after *count are left untouched.  `bits` is
+// the number of low key bits that can be non-zero.  The sorted pairs end in
+// keys/vals; keys_tmp/vals_tmp are scratch of the same capacity.
+cudaError_t sort_pairs_u64(uint64_t *keys, uint64_t *keys_tmp, int *vals, int *vals_tmp,
+                           const int *count, int64_t capacity, int bits, SortScratch &s,
+                           cudaStream_t st);
+cudaError_t sort_pairs_u32(uint32_t *keys, uint32_t *keys_tmp, int *vals, int *vals_tmp,
+                           const int *count, int64_t capacity, int bits, SortScratch &s,
+                           cudaStream_t st);
+
+// ---------------------------------------------------------------- hierarchy
+struct TreeBuffers {
+  int64_t capacity = 0;   // items
+  int64_t leaves_cap = 0; // power of two >= capacity
+  float4 *lo = nullptr, *hi = nullptr;  // [2 * leaves_cap]
+  int *ids = nullptr, *ids_tmp = nullptr;
+  uint64_t *keys = nullptr, *keys_tmp = nullptr;
+  int *flags = nullptr;   // [leaves_cap]
+  int *size = nullptr;    // device scalar: leaves of the current build
+  int *count = nullptr;   // device scalar: items of the current build
+  Tree tree() const { return Tree{lo, hi, ids, size}; }
+};
+
+cudaError_t tree_alloc(TreeBuffers &t, int64_t capacity);
+void tree_free(TreeBuffers &t);
+// Build over item boxes [0, *count).  `count_ptr` null means `static_count`.
+// `layered` adds lo.z (a layer number) above the Morton bits (kernels.py:89-90).
+cudaError_t tree_build(TreeBuffers &t, const float4 *lo, const float4 *hi, const int *count_ptr,
+                       int static_count, bool layered, SortScratch &s, cudaStream_t st);
+
+}  // namespace edp
+
+namespace edp {
+
+// Pool capacities of an extraction (warp_peel/events.py:19-33, solver.py:10-31).
+struct Caps {
+  int64_t frontier, regions, hits, vertices, triangles, rounds, layers, edge_vertices;
+};
+
+// Device scalars kept between kernels of one extraction.
+enum Scalar : int {
+  kLivePolygons = 0,   // min(status[2], regions)
+  kPatchEdges = 1,     // patch edges of all live polygons
+  kLiveHits = 2,       // min(metrics[5], hits)
+  kLiveVertices = 3,   // min(status[6], vertices)
+  kSourceCount = 4,    // n (constant)
+  kSegmentCount = 5,   // 8 n (constant)
+  kFrontierLive = 6,   // min(status[0], frontier)
+  kScalarCount = 16
+};
+
+// Every device pointer of a workspace, passed by value to the kernels.
+struct Dev {
+  const double *vertices;
+  const int *faces;
+  const double *camera;
+  const double *settings;
+  int nv, n;
+  int limit, all_layers, share_regions, propagate_ranks, merge_regions;
+  Caps cap;
+
+  int *status;
+  long long *metrics;
+  int *sc;
+  int *parity;
+  int *condition;
+  double *inverse;  // 4x4 row-major camera inverse
+
+  // welding
+  int *canonical, *weld_table, *weld_min, *weld_slot;
+  int weld_mask;
+  // projected sources, at most kSourceVertices vertices each
+  V2 *src_v;
+  int *src_n;
+  Plane *scores;
+  int *facing, *clipped;
+  float4 *src_lo, *src_hi;
+  // undirected mesh edges
+  unsigned long long *ekey_table;
+  int *ekey_count, *ekey_member, *edge_slot, *masks;
+  unsigned long long *edge_keys;  // welded edge key of each face edge (topology owner)
+  int ekey_mask;
+  // contour segments: kSourceVertices slots per source
+  V2 *seg_a, *seg_b;
+  double *seg_za, *seg_zb;  // per table slot: minimum endpoint depths
+  V2 *seg_near;             // per representative segment: (near depth a, near depth b)
+  float4 *seg_lo, *seg_hi;
+  int *seg_table, *seg_min, *seg_slot;
+  int seg_mask;
+  Tree source_tree, seg_tree, point_tree;
+  // frontier ping-pong
+  V2 *fv[2];
+  int *fn[2], *fsrc[2], *fcur[2];
+  // output polygons
+  V2 *out_v;
+  int *out_n, *out_src, *out_layer;
+  // patch connectivity
+  int *counts, *offsets;
+  int2 *tasks;
+  unsigned long long *owners;
+  V2 *starts, *ends;
+  int *partners, *edge_hash, *parents, *reps;
+  int edge_hash_mask;
+  // samples and query groups
+  V2 *samples;
+  int *groups, *sample_table, *sample_min, *sample_slot;
+  int sample_mask;
+  double *cell_bounds;  // [1024][4]
+  int *cell_min, *cell_valid;
+  int2 *heavy_beams, *heavy_queries;
+  // shared ray hits
+  double *hit_depth;
+  int *hit_src, *hit_group, *hit_ids, *hit_ids_tmp;
+  unsigned long long *hkeys, *hkeys_tmp;
+  int *group_counts, *group_offsets;
+  // boundary noding and triangles
+  V2 *bverts;
+  int *blayers;
+  float4 *pt_lo, *pt_hi;
+  int2 *mtasks;
+  V2 *tri_uv;        // [triangles][3]
+  double *tri_world; // [triangles][3][3]
+  int *tri_src, *tri_layer;
+  unsigned long long cond_handle;  // cudaGraphConditionalHandle of the subdivision loop
+  int use_handle;
+};
+
+// Stage launchers (edp_kernels.cu).  Each enqueues kernels on `st`.
+cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                          TreeBuffers &seg_tree, cudaStream_t st);
+cudaError_t stage_step(const Dev &d, cudaStream_t st);
+cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st);
+cudaError_t stage_mesh(const Dev &d, SortScratch &s, TreeBuffers &point_tree, cudaStream_t st);
+
+}  // namespace edp

@@ -1,0 +1,172 @@
+// Mesh stage: boundary vertex gathering, the layered point hierarchy and
+// per-edge noding, centroid-fan triangulation and world lifting
+// (warp_peel/kernels.py:941-1204, events.py:720-780).
+#include "edp_internal.h"
+
+namespace edp {
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kMaxEdgeVertices = 128;  // edge noding capacity (solver.py:140-143)
+
+__device__ inline int64_t tid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
+__device__ inline int64_t stride() { return int64_t(gridDim.x) * blockDim.x; }
+
+__global__ void k_mesh_counts(Dev d) {
+  const int live = d.sc[kLivePolygons];
+  for (int64_t i = tid(); i < live; i += stride())
+    d.counts[i] = d.status[kError] == 0 ? d.out_n[i] : 0;
+}
+
+__global__ void k_mesh_check(Dev d) {
+  int total = d.sc[kLiveVertices];
+  d.status[kBoundaryVertices] = total;
+  if (int64_t(total) > d.cap.vertices) {
+    set_error(d.status, kErrVertices);
+    d.sc[kLiveVertices] = int(d.cap.vertices);
+  }
+}
+
+// Boundary vertices with their layer, one noding task per polygon edge, and
+// the vertices' point boxes at z = layer (kernels.py:953-991, event_kernels.py:504-516).
+__global__ void k_scatter(Dev d) {
+  const int live = d.sc[kLivePolygons];
+  for (int64_t i = tid(); i < live; i += stride()) {
+    if (d.status[kError] != 0) return;
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    const int n = d.out_n[i], layer = d.out_layer[i];
+    for (int j = 0; j < n; ++j) {
+      int64_t slot = int64_t(d.offsets[i]) + j;
+      if (slot >= d.cap.vertices) break;
+      V2 x = p[j];
+      d.bverts[slot] = x;
+      d.blayers[slot] = layer;
+      d.mtasks[slot] = make_int2(int(i), j);
+      d.pt_lo[slot] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
+                                  float(layer), 0.f);
+      d.pt_hi[slot] = make_float4(__double2float_ru(x.x + 2.0e-7), __double2float_ru(x.y + 2.0e-7),
+                                  float(layer), 0.f);
+    }
+  }
+}
+
+// World position of a window point on a source plane (kernels.py:994-1006).
+__device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
+  const double *st = d.settings, *m = d.inverse;
+  double u = st[0] + x.x * (st[2] - st[0]);
+  double v = st[1] + x.y * (st[3] - st[1]);
+  double z = value(s, x);
+  if (st[4] != 0.0) {
+    z = -1.0 / z;
+    u *= z;
+    v *= z;
+  }
+  for (int r = 0; r < 3; ++r) w[r] = m[4 * r] * u + m[4 * r + 1] * v + m[4 * r + 2] * z + m[4 * r + 3];
+}
+
+// Node one polygon edge against every same-layer boundary vertex lying on it
+// (collinear within EPS, strictly inside the edge), sort the split
+// parameters, and emit centroid-fan triangles lifted to world space
+// (kernels.py:1009-1125).
+__global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity) {
+  const int tasks = d.sc[kLiveVertices];
+  const int leaves = *d.point_tree.size;
+  double params[kMaxEdgeVertices];
+  for (int64_t t = tid(); t < tasks; t += stride()) {
+    if (d.status[kError] != 0) return;
+    const int2 task = d.mtasks[t];
+    const int i = task.x, edge = task.y;
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    const int n = d.out_n[i];
+    if (edge >= n) continue;
+    const int layer = d.out_layer[i], source = d.out_src[i];
+    V2 a = p[edge], b = p[(edge + 1) % n], dir = b - a;
+    double length2 = dot(dir, dir);
+    V2 center = v2(0.0, 0.0);
+    for (int j = 0; j < n; ++j) center = center + p[j] / double(n);
+    float4 lo = make_float4(__double2float_rd(fmin(a.x, b.x) - 2.0e-7),
+                            __double2float_rd(fmin(a.y, b.y) - 2.0e-7), float(layer), 0.f);
+    float4 hi = make_float4(__double2float_ru(fmax(a.x, b.x) + 2.0e-7),
+                            __double2float_ru(fmax(a.y, b.y) + 2.0e-7), float(layer), 0.f);
+    int count = 0, node = 1;
+    bool overflow = false;
+    const double tol = kEps * sqrt(length2);
+    while (node > 0 && length2 > 0.0) {
+      int j;
+      node = query_next(d.point_tree, leaves, lo, hi, node, 0, j);
+      if (j < 0) break;
+      V2 x = d.bverts[j];
+      double tt = dot(x - a, dir) / length2;
+      if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= tol) {
+        if (count < edge_capacity) {
+          params[count++] = tt;
+        } else {
+          overflow = true;
+          break;
+        }
+      }
+    }
+    if (overflow) {
+      set_error(d.status, kErrEdgeNoding);
+      return;
+    }
+    // Insertion sort: edges carry few split points; the bound is edge_capacity.
+    for (int k = 1; k < count; ++k) {
+      double v = params[k];
+      int m = k - 1;
+      while (m >= 0 && params[m] > v) {
+        params[m + 1] = params[m];
+        --m;
+      }
+      params[m + 1] = v;
+    }
+    const Plane sc = d.scores[source];
+    double previous = 0.0;
+    V2 cursor = a;
+    for (int step = 0; step <= count; ++step) {
+      double following = step < count ? params[step] : 1.0;
+      if (following <= previous + kEps) continue;
+      V2 next = a + following * dir;
+      if (fabs(cross(center, cursor, next)) > kEps * kEps) {
+        int slot = atomicAdd(&d.status[kTriangles], 1);
+        if (slot < d.cap.triangles) {
+          V2 *uv = d.tri_uv + 3 * int64_t(slot);
+          double *w = d.tri_world + 9 * int64_t(slot);
+          uv[0] = center;
+          uv[1] = cursor;
+          uv[2] = next;
+          lift(d, center, sc, w);
+          lift(d, cursor, sc, w + 3);
+          lift(d, next, sc, w + 6);
+          d.tri_src[slot] = source;
+          d.tri_layer[slot] = layer;
+        } else {
+          set_error(d.status, kErrTriangles);
+        }
+      }
+      cursor = next;
+      previous = following;
+    }
+  }
+}
+
+unsigned blocks(int64_t n) {
+  int64_t g = ceil_div(n > 0 ? n : 1, kBlock);
+  return unsigned(g < 148 * 16 ? g : 148 * 16);
+}
+
+}  // namespace
+
+cudaError_t stage_mesh(const Dev &d, SortScratch &s, TreeBuffers &point_tree, cudaStream_t st) {
+  const int64_t R = d.cap.regions, E = d.cap.vertices;
+  k_mesh_counts<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
+  k_mesh_check<<<1, 1, 0, st>>>(d);
+  k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kLiveVertices, 0, true, s, st));
+  int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
+  k_mesh_edges<<<blocks(E), kBlock, 0, st>>>(d, cap);
+  return cudaGetLastError();
+}
+
+}  // namespace edp

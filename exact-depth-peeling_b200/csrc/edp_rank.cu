@@ -1,0 +1,584 @@
+// Rank stage: certified patch connectivity, canonical samples, shared query
+// groups with certified rectangles, ray hit gathering, the stable hit order
+// and per-polygon rank assignment (warp_peel/events.py:291-635,
+// components.py, beams.py, event_kernels.py:28-385).
+#include "edp_internal.h"
+
+namespace edp {
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kHeavyWorkers = 8192;  // persistent continuation workers (events.py:510,564)
+constexpr int kCells = 1024;         // 32 x 32 image buckets (beams.py:18-22)
+
+__device__ inline int64_t tid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
+__device__ inline int64_t stride() { return int64_t(gridDim.x) * blockDim.x; }
+__device__ inline void add_metric(const Dev &d, int m, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[m]),
+            static_cast<unsigned long long>(v));
+}
+__device__ inline int live_polygons(const Dev &d) { return d.sc[kLivePolygons]; }
+__device__ inline float lower_f(double x) { return __double2float_rd(x); }
+__device__ inline float upper_f(double x) { return __double2float_ru(x); }
+
+__global__ void k_rank_begin(Dev d) {
+  d.sc[kLivePolygons] = int(min(int64_t(d.status[kPolygons]), d.cap.regions));
+}
+
+__global__ void k_polygon_init(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    d.counts[i] = d.out_n[i];
+    d.parents[i] = int(i);
+    d.group_counts[i] = 0;
+  }
+}
+
+__global__ void k_check_edges(Dev d) {
+  int total = d.sc[kPatchEdges];
+  if (int64_t(total) > d.cap.vertices) {
+    set_error(d.status, kErrVertices);
+    d.sc[kPatchEdges] = int(d.cap.vertices);
+  }
+}
+
+// Owner of each patch edge: the welded mesh edge when the patch edge lies on
+// an internal (non-contour) edge of its unclipped source, else the source
+// itself (components.py:287-327).
+__global__ void k_patch_edges(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    if (d.status[kError] != 0) return;
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    const int n = d.out_n[i], source = d.out_src[i];
+    const V2 *q = d.src_v + int64_t(kSourceVertices) * source;
+    const int qn = d.src_n[source];
+    for (int k = 0; k < n; ++k) {
+      int64_t slot = int64_t(d.offsets[i]) + k;
+      if (slot >= d.cap.vertices) break;
+      V2 a = p[k], b = p[(k + 1) % n];
+      unsigned long long owner = 0x8000000000000000ull | static_cast<unsigned>(source);
+      if (d.clipped[source] == 0) {
+        for (int j = 0; j < qn; ++j) {
+          int edge = d.facing[source] < 0 ? (4 - j) % 3 : j;
+          if (d.masks[3 * int64_t(source) + edge] == 0) {
+            V2 u = q[j], v = q[(j + 1) % qn];
+            if ((a == u || a == v || cross(u, v, a) == 0.0) &&
+                (b == u || b == v || cross(u, v, b) == 0.0)) {
+              owner = d.edge_keys[3 * int64_t(source) + edge];
+              break;
+            }
+          }
+        }
+      }
+      d.owners[slot] = owner;
+      d.starts[slot] = a;
+      d.ends[slot] = b;
+      d.tasks[slot] = make_int2(int(i), k);
+      d.partners[slot] = -1;
+    }
+  }
+}
+
+__device__ inline uint64_t point_key(V2 x) {
+  return mix64(key_bits(x.x)) ^ mix64(key_bits(x.y) + 19ull);
+}
+
+// A bounded open-addressing table pairs each patch edge with the reversed edge
+// of another patch that has the same owner (components.py:330-366).  The key
+// is symmetric in the endpoints so both directions probe the same chain.
+__global__ void k_match_edges(Dev d) {
+  const int total = d.sc[kPatchEdges];
+  for (int64_t i = tid(); i < total; i += stride()) {
+    if (d.status[kError] != 0) return;
+    V2 a = d.starts[i], b = d.ends[i];
+    if (a == b) continue;
+    const unsigned long long owner = d.owners[i];
+    uint64_t key = mix64(owner) ^ point_key(a) ^ point_key(b);
+    uint32_t slot = uint32_t(key) & uint32_t(d.edge_hash_mask);
+    bool placed = false;
+    for (int attempt = 0; attempt < 64; ++attempt) {
+      int other = atomicCAS(&d.edge_hash[slot], -1, int(i));
+      if (other < 0) {
+        placed = true;
+        break;
+      }
+      if (d.owners[other] == owner && d.tasks[i].x != d.tasks[other].x && a == d.ends[other] &&
+          b == d.starts[other]) {
+        d.partners[i] = other;
+        d.partners[other] = int(i);
+        add_metric(d, kMatchedPatchEdges, 1);
+        placed = true;
+        break;
+      }
+      slot = (slot + 1) & uint32_t(d.edge_hash_mask);
+    }
+    if (!placed) add_metric(d, kEdgeHashMisses, 1);  // loses only the optimisation
+  }
+}
+
+__device__ inline int uf_read(int *p, int i) { return *reinterpret_cast<volatile int *>(p + i); }
+
+// Lock-free union-find with atomic-min links (components.py:369-390).
+__device__ inline int uf_root(int *parents, int i) {
+  int node = i;
+  while (true) {
+    int parent = uf_read(parents, node);
+    if (parent == node) break;
+    int grand = uf_read(parents, parent);
+    atomicMin(&parents[node], grand);
+    node = grand;
+  }
+  return node;
+}
+
+__device__ inline void uf_unite(int *parents, int a, int b) {
+  int ra = uf_root(parents, a), rb = uf_root(parents, b);
+  while (ra != rb) {
+    int high = max(ra, rb), low = min(ra, rb);
+    int old = atomicMin(&parents[high], low);
+    if (old == high) break;
+    ra = uf_root(parents, old);
+    rb = uf_root(parents, low);
+  }
+}
+
+// Matched edges are connected when no nearer-or-equal contour passes through
+// the edge midpoint (components.py:393-450).
+__global__ void k_connect(Dev d) {
+  const int total = d.sc[kPatchEdges];
+  const int leaves = *d.seg_tree.size;
+  for (int64_t i = tid(); i < total; i += stride()) {
+    if (d.status[kError] != 0) return;
+    int other = d.partners[i];
+    if (other <= i) continue;
+    int2 task = d.tasks[i];
+    V2 a = d.starts[i], b = d.ends[i];
+    if (length(b - a) <= 16.0 * kEps) continue;
+    V2 x = 0.5 * (a + b);
+    double z = value(d.scores[d.out_src[task.x]], x);
+    double pad = 2.0e-7 * fmax(1.0, fabs(z));
+    float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
+    float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), upper_f(z + pad), 0.f);
+    int node = 1, visits = 0;
+    bool safe = true;
+    while (node > 0) {
+      int c;
+      node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
+      if (c < 0) break;
+      ++visits;
+      V2 u = d.seg_a[c], v = d.seg_b[c], dv = v - u;
+      double len = length(dv);
+      if (len > 0.0) {
+        double t = dot(x - u, dv) / dot(dv, dv);
+        if (fabs(cross(u, v, x)) <= kEps * len && t >= -kEps / len && t <= 1.0 + kEps / len) {
+          V2 near = d.seg_near[c];
+          double depth = near.x + t * (near.y - near.x);
+          if (depth <= z + pad) {
+            safe = false;
+            break;
+          }
+        }
+      }
+    }
+    add_metric(d, kConnectionContourTests, visits);
+    if (safe) {
+      uf_unite(d.parents, task.x, d.tasks[other].x);
+      add_metric(d, kRankConnections, 1);
+    }
+  }
+}
+
+__global__ void k_roots(Dev d, int connected) {
+  const int live = live_polygons(d);
+  int components = 0;
+  for (int64_t i = tid(); i < live; i += stride()) {
+    int r = connected ? uf_root(d.parents, int(i)) : int(i);
+    d.reps[i] = r;
+    components += r == int(i);
+  }
+  if (components) add_metric(d, kRankComponents, d.propagate_ranks ? components : 0);
+}
+
+// Canonical interior sample of each polygon's representative: the vertex mean
+// accumulated from the lexicographically smallest vertex, so that rotated
+// copies of one footprint share bit-identical samples (event_kernels.py:28-48).
+__global__ void k_samples(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    int r = d.reps[i];
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * r;
+    int n = d.out_n[r];
+    int anchor = 0;
+    for (int j = 1; j < n; ++j)
+      if (less(p[j], p[anchor])) anchor = j;
+    V2 x = v2(0.0, 0.0);
+    for (int j = 0; j < n; ++j) x = x + p[(anchor + j) % n] / double(n);
+    d.samples[i] = x;
+  }
+}
+
+__device__ inline int cell_of(V2 x) {
+  int cx = int(fmin(fmax(x.x * 32.0, 0.0), 31.0)), cy = int(fmin(fmax(x.y * 32.0, 0.0), 31.0));
+  return cx * 32 + cy;
+}
+
+// Identical samples form one query group, whose id is the smallest polygon
+// index in it (the reference groups by sorted position, event_kernels.py:71-92).
+// Each 32x32 image cell also gathers its samples' bounding rectangle as a
+// sharing proposal (beams.py:49-86).
+__global__ void k_group_insert(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    V2 x = d.samples[i];
+    uint32_t slot = uint32_t(point_key(x)) & uint32_t(d.sample_mask);
+    for (int probe = 0; probe <= d.sample_mask; ++probe) {
+      int cur = atomicCAS(&d.sample_table[slot], -1, int(i));
+      if (cur == -1 || d.samples[cur] == x) break;
+      slot = (slot + 1) & uint32_t(d.sample_mask);
+    }
+    atomicMin(&d.sample_min[slot], int(i));
+    d.sample_slot[i] = int(slot);
+    if (d.share_regions) {
+      int c = cell_of(x);
+      atomicMin(&d.cell_min[c], int(i));
+      atomic_min_double(&d.cell_bounds[4 * c + 0], x.x);
+      atomic_min_double(&d.cell_bounds[4 * c + 1], x.y);
+      atomic_max_double(&d.cell_bounds[4 * c + 2], x.x);
+      atomic_max_double(&d.cell_bounds[4 * c + 3], x.y);
+    }
+  }
+}
+
+__global__ void k_group_resolve(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) d.groups[i] = d.sample_min[d.sample_slot[i]];
+}
+
+__global__ void k_cells_reset(Dev d) {
+  int c = int(tid());
+  if (c < kCells) {
+    d.cell_min[c] = 0x7fffffff;
+    d.cell_valid[c] = 0;
+    d.cell_bounds[4 * c + 0] = 1.0e30;
+    d.cell_bounds[4 * c + 1] = 1.0e30;
+    d.cell_bounds[4 * c + 2] = -1.0e30;
+    d.cell_bounds[4 * c + 3] = -1.0e30;
+  }
+}
+
+// Source polygon strictly covers the four corners of cell c's rectangle with
+// an edge-length margin (beams.py:89-98).
+__device__ inline bool covers(const Dev &d, int source, int c) {
+  const V2 *p = d.src_v + int64_t(kSourceVertices) * source;
+  const int n = d.src_n[source];
+  const double *b = d.cell_bounds + 4 * c;
+  for (int j = 0; j < n; ++j) {
+    V2 u = p[j], v = p[(j + 1) % n];
+    double margin = kEps * length(v - u);
+    for (int k = 0; k < 4; ++k) {
+      V2 x = v2(b[2 * (k % 2)], b[1 + 2 * (k / 2)]);
+      if (cross(u, v, x) <= margin) return false;
+    }
+  }
+  return n > 0;
+}
+
+__device__ inline void cell_box(const Dev &d, int c, float4 &lo, float4 &hi) {
+  const double *b = d.cell_bounds + 4 * c;
+  lo = make_float4(lower_f(b[0] - 2.0e-7), lower_f(b[1] - 2.0e-7), -1.0e30f, 0.f);
+  hi = make_float4(upper_f(b[2] + 2.0e-7), upper_f(b[3] + 2.0e-7), 1.0e30f, 0.f);
+}
+
+// Certified rectangles: a cell's samples may share one ray group only if
+// every source candidate strictly covers the cell's sample rectangle; on
+// intersection-resolved input the covering set and its depth order are then
+// constant over the rectangle (beams.py:109-146).
+__global__ void k_certify(Dev d) {
+  const int c = int(tid());
+  if (c >= kCells || d.status[kError] != 0 || d.cell_min[c] == 0x7fffffff) return;
+  const double *b = d.cell_bounds + 4 * c;
+  if (b[0] == b[2] && b[1] == b[3]) return;  // identical samples already share
+  add_metric(d, kBeamAttempts, 1);
+  float4 lo, hi;
+  cell_box(d, c, lo, hi);
+  const int leaves = *d.source_tree.size;
+  int node = 1, visits = 0, accepted = 1;
+  for (int step = 0; step < kCandidatesPerPass; ++step) {
+    int s;
+    node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
+    if (s < 0) break;
+    ++visits;
+    if (!covers(d, s, c)) {
+      accepted = 0;
+      break;
+    }
+    if (node == 0) break;
+  }
+  add_metric(d, kBeamCandidateTests, visits);
+  d.cell_valid[c] = accepted;
+  if (accepted && node > 0) {
+    while (node < leaves) node *= 2;
+    int slot = int(atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kHeavyBeams]), 1ull));
+    d.heavy_beams[slot] = make_int2(c, node);
+  }
+}
+
+// Disjoint-subtree partition of the unvisited traversal suffixes of long
+// queries (event_kernels.py:248-298, beams.py:149-188).
+__device__ inline void heavy_partition(int leaves, long long jobs, int &parts, int &width) {
+  parts = min(8192, leaves);
+  while (parts > 16 && (long long)parts * jobs > 65536) parts /= 2;
+  width = leaves / parts;
+}
+
+__global__ void k_certify_heavy(Dev d) {
+  if (d.status[kError] != 0) return;
+  const int leaves = *d.source_tree.size;
+  const long long jobs = d.metrics[kHeavyBeams];
+  int parts, width;
+  heavy_partition(leaves, jobs, parts, width);
+  for (long long task = tid(); task < jobs * parts; task += stride()) {
+    int2 job = d.heavy_beams[task / parts];
+    int part = int(task % parts), c = job.x;
+    int first = leaves + part * width;
+    if (job.y >= first + width || atomicAdd(&d.cell_valid[c], 0) == 0) continue;
+    int root = parts + part, node = job.y > first ? job.y : root, end = successor(root);
+    float4 lo, hi;
+    cell_box(d, c, lo, hi);
+    int visits = 0;
+    while (node > 0 && node != end) {
+      int s;
+      node = query_next(d.source_tree, leaves, lo, hi, node, end, s);
+      if (s < 0) break;
+      ++visits;
+      if (!covers(d, s, c)) {
+        atomicMin(&d.cell_valid[c], 0);
+        break;
+      }
+    }
+    add_metric(d, kBeamCandidateTests, visits);
+  }
+}
+
+__global__ void k_apply_cells(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    int c = cell_of(d.samples[i]);
+    if (d.cell_valid[c] != 0) {
+      int root = d.cell_min[c];
+      d.groups[i] = root;
+      if (root == int(i)) add_metric(d, kCertifiedBeams, 1);
+    }
+  }
+}
+
+// Half-open containment: a point on an edge belongs to the polygon only if the
+// edge is "owned" (rising, or horizontal running in -x), so a tessellated
+// sheet counts once on shared edges (event_kernels.py:95-148).
+__device__ inline bool contains_flat(const Dev &d, int source, V2 x) {
+  const V2 *p = d.src_v + int64_t(kSourceVertices) * source;
+  const int n = d.src_n[source];
+  for (int j = 0; j < n; ++j) {
+    V2 a = p[j], b = p[(j + 1) % n];
+    double s = cross(a, b, x);
+    bool owned = b.y > a.y || (b.y == a.y && b.x < a.x);
+    if (s < 0.0 || (s == 0.0 && !owned)) return false;
+  }
+  return n > 0;
+}
+
+__device__ inline void store_hit(const Dev &d, int source, int group, V2 x) {
+  long long slot = (long long)atomicAdd(
+      reinterpret_cast<unsigned long long *>(&d.metrics[kRayHits]), 1ull);
+  if (slot < d.cap.hits) {
+    d.hit_depth[slot] = value(d.scores[source], x);
+    d.hit_src[slot] = source;
+    d.hit_group[slot] = group;
+  } else {
+    set_error(d.status, kErrHits);
+  }
+}
+
+// One ray per group leader: up to kCandidatesPerPass sources, the rest of the
+// traversal is queued for the persistent continuation (event_kernels.py:196-245).
+__global__ void k_ray_hits(Dev d) {
+  const int live = live_polygons(d);
+  const int leaves = *d.source_tree.size;
+  for (int64_t i = tid(); i < live; i += stride()) {
+    if (d.status[kError] != 0) return;
+    if (d.groups[i] != int(i)) continue;
+    V2 x = d.samples[i];
+    float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
+    float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
+    int node = 1, count = 0, visits = 0;
+    for (int step = 0; step < kCandidatesPerPass; ++step) {
+      int s;
+      node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
+      if (s < 0) break;
+      ++visits;
+      if (contains_flat(d, s, x)) {
+        store_hit(d, s, int(i), x);
+        ++count;
+      }
+      if (node == 0) break;
+    }
+    atomicAdd(&d.group_counts[i], count);
+    add_metric(d, kRayGroups, 1);
+    add_metric(d, kRayCandidateTests, visits);
+    if (node > 0) {
+      while (node < leaves) node *= 2;
+      int slot = int(atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kHeavyRayGroups]), 1ull));
+      d.heavy_queries[slot] = make_int2(int(i), node);
+    }
+  }
+}
+
+__global__ void k_heavy_hits(Dev d) {
+  if (d.status[kError] != 0) return;
+  const int leaves = *d.source_tree.size;
+  const long long jobs = d.metrics[kHeavyRayGroups];
+  int parts, width;
+  heavy_partition(leaves, jobs, parts, width);
+  for (long long task = tid(); task < jobs * parts; task += stride()) {
+    int2 job = d.heavy_queries[task / parts];
+    int part = int(task % parts);
+    int first = leaves + part * width;
+    if (job.y >= first + width) continue;
+    int root = parts + part, node = job.y > first ? job.y : root, end = successor(root);
+    const int i = job.x;
+    V2 x = d.samples[i];
+    float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
+    float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
+    int count = 0, visits = 0;
+    while (node > 0 && node != end) {
+      int s;
+      node = query_next(d.source_tree, leaves, lo, hi, node, end, s);
+      if (s < 0) break;
+      ++visits;
+      if (contains_flat(d, s, x)) {
+        store_hit(d, s, i, x);
+        ++count;
+      }
+    }
+    if (count) atomicAdd(&d.group_counts[i], count);
+    add_metric(d, kRayCandidateTests, visits);
+  }
+}
+
+__global__ void k_check_hits(Dev d) {
+  long long total = d.metrics[kRayHits];
+  if (total > d.cap.hits) set_error(d.status, kErrHits);
+  d.sc[kLiveHits] = int(min(total, (long long)d.cap.hits));
+}
+
+// Keys of the three stable passes that order hits by (group, depth, source)
+// (event_kernels.py:313-339, events.py:701-718).
+__global__ void k_hit_keys(Dev d, int stage) {
+  const int live = d.sc[kLiveHits];
+  for (int64_t i = tid(); i < live; i += stride()) {
+    int h = stage == 0 ? int(i) : d.hit_ids[i];
+    if (stage == 0) d.hit_ids[i] = int(i);
+    unsigned long long key;
+    if (stage == 0)
+      key = static_cast<unsigned>(d.hit_src[h]);
+    else if (stage == 1)
+      key = ordered_bits(d.hit_depth[h]);
+    else
+      key = static_cast<unsigned>(d.hit_group[h]);
+    d.hkeys[i] = key;
+  }
+}
+
+// Rank = number of the group's hits nearer than the representative's source
+// at this polygon's sample, equal depths ordered by source index
+// (event_kernels.py:342-385).
+__global__ void k_assign(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    if (d.status[kError] != 0) return;
+    int source = d.out_src[d.reps[i]];
+    V2 x = d.samples[i];
+    double z = value(d.scores[source], x);
+    int g = d.groups[i];
+    int low = 0, high = d.group_counts[g];
+    const int *ids = d.hit_ids + d.group_offsets[g];
+    while (low < high) {
+      int mid = (low + high) / 2;
+      int h = ids[mid];
+      int hs = d.hit_src[h];
+      double hz = value(d.scores[hs], x);
+      if (hz < z || (hz == z && hs < source))
+        low = mid + 1;
+      else
+        high = mid;
+    }
+    d.out_layer[i] = low;
+    if (low >= d.limit) {
+      if (d.all_layers)
+        set_error(d.status, kErrLayers);
+      else
+        d.out_n[i] = 0;
+    } else {
+      atomicMax(&d.status[kLayers], low + 1);
+    }
+  }
+}
+
+__global__ void k_layers_reset(Dev d) { d.status[kLayers] = 0; }
+
+unsigned blocks(int64_t n) {
+  int64_t g = ceil_div(n > 0 ? n : 1, kBlock);
+  return unsigned(g < 148 * 16 ? g : 148 * 16);
+}
+
+int bits_for(int64_t n) {
+  int b = 1;
+  while ((int64_t(1) << b) < n + 1) ++b;
+  return b;
+}
+
+}  // namespace
+
+cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
+  const int64_t R = d.cap.regions, E = d.cap.vertices;
+  k_rank_begin<<<1, 1, 0, st>>>(d);
+  k_polygon_init<<<blocks(R), kBlock, 0, st>>>(d);
+  const bool connected = d.propagate_ranks || d.merge_regions;
+  if (connected) {
+    EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kPatchEdges, s, st));
+    k_check_edges<<<1, 1, 0, st>>>(d);
+    k_patch_edges<<<blocks(R), kBlock, 0, st>>>(d);
+    EDP_CHECK(cudaMemsetAsync(d.edge_hash, 0xff, sizeof(int) * (int64_t(d.edge_hash_mask) + 1), st));
+    k_match_edges<<<blocks(E), kBlock, 0, st>>>(d);
+    if (d.propagate_ranks) k_connect<<<blocks(E), kBlock, 0, st>>>(d);
+  }
+  k_roots<<<blocks(R), kBlock, 0, st>>>(d, d.propagate_ranks ? 1 : 0);
+  k_samples<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_CHECK(cudaMemsetAsync(d.sample_table, 0xff, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
+  EDP_CHECK(cudaMemsetAsync(d.sample_min, 0x7f, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
+  k_cells_reset<<<kCells / 128, 128, 0, st>>>(d);
+  k_group_insert<<<blocks(R), kBlock, 0, st>>>(d);
+  k_group_resolve<<<blocks(R), kBlock, 0, st>>>(d);
+  if (d.share_regions) {
+    k_certify<<<kCells / 128, 128, 0, st>>>(d);
+    k_certify_heavy<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+    k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
+  }
+  k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
+  k_heavy_hits<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+  EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
+  k_check_hits<<<1, 1, 0, st>>>(d);
+  const int pass_bits[3] = {bits_for(d.n), 64, bits_for(R)};
+  for (int stage = 0; stage < 3; ++stage) {
+    k_hit_keys<<<blocks(d.cap.hits), kBlock, 0, st>>>(d, stage);
+    EDP_CHECK(sort_pairs_u64(reinterpret_cast<uint64_t *>(d.hkeys),
+                             reinterpret_cast<uint64_t *>(d.hkeys_tmp), d.hit_ids, d.hit_ids_tmp,
+                             d.sc + kLiveHits, d.cap.hits, pass_bits[stage], s, st));
+  }
+  k_layers_reset<<<1, 1, 0, st>>>(d);
+  k_assign<<<blocks(R), kBlock, 0, st>>>(d);
+  return cudaGetLastError();
+}
+
+}  // namespace edp

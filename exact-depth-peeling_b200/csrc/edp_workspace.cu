@@ -1,0 +1,420 @@
+// Workspace lifetime, stage orchestration, CUDA graph capture with a device
+// conditional loop, and the C ABI declared in include/edp.h.
+#include <cstring>
+#include <initializer_list>
+#include <vector>
+
+#include "../../include/edp.h"
+#include "edp_internal.h"
+
+using namespace edp;
+
+struct edp_peeler {
+  int method = 0;  // 0 = EventPeeler, 1 = DevicePeeler
+  Dev d{};
+  cudaStream_t stream = nullptr;
+  cudaStream_t body_stream = nullptr;
+  SortScratch scratch;
+  TreeBuffers source_tree, seg_tree, point_tree;
+  std::vector<void *> allocations;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool warmed = false;
+  int device = 0;
+};
+
+namespace {
+
+thread_local int g_last_cuda = 0;
+
+int cuda_fail(cudaError_t e) {
+  g_last_cuda = int(e);
+  return EDP_ERR_CUDA;
+}
+
+#define EDP_TRY(call)                                   \
+  do {                                                  \
+    cudaError_t e__ = (call);                           \
+    if (e__ != cudaSuccess) return cuda_fail(e__);      \
+  } while (0)
+
+template <class T>
+cudaError_t alloc(edp_peeler *p, T **ptr, int64_t count) {
+  if (count < 1) count = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(T) * size_t(count));
+  if (e == cudaSuccess) {
+    p->allocations.push_back(*ptr);
+    e = cudaMemset(*ptr, 0, sizeof(T) * size_t(count));
+  }
+  return e;
+}
+
+int table_mask(int64_t entries) { return int(pow2_at_least(2 * (entries > 0 ? entries : 1)) - 1); }
+
+bool caps_valid(const Caps &c) {
+  const int64_t v[] = {c.frontier, c.regions, c.hits, c.vertices, c.triangles, c.rounds, c.layers,
+                       c.edge_vertices};
+  for (int64_t x : v)
+    if (x < 1 || x > (int64_t(1) << 30)) return false;
+  return c.edge_vertices <= 128;
+}
+
+cudaError_t allocate_event(edp_peeler *p) {
+  Dev &d = p->d;
+  const int64_t n = d.n, nv = d.nv, F = d.cap.frontier, R = d.cap.regions, H = d.cap.hits,
+                E = d.cap.vertices, T = d.cap.triangles, S = int64_t(kSourceVertices) * n;
+  EDP_CHECK(alloc(p, &d.status, kStatusSlots));
+  EDP_CHECK(alloc(p, &d.metrics, kMetrics));
+  EDP_CHECK(alloc(p, &d.sc, kScalarCount));
+  EDP_CHECK(alloc(p, &d.parity, 1));
+  EDP_CHECK(alloc(p, &d.condition, 1));
+  EDP_CHECK(alloc(p, &d.inverse, 16));
+  d.weld_mask = table_mask(nv);
+  EDP_CHECK(alloc(p, &d.canonical, nv));
+  EDP_CHECK(alloc(p, &d.weld_slot, nv));
+  EDP_CHECK(alloc(p, &d.weld_table, int64_t(d.weld_mask) + 1));
+  EDP_CHECK(alloc(p, &d.weld_min, int64_t(d.weld_mask) + 1));
+  EDP_CHECK(alloc(p, &d.src_v, S));
+  EDP_CHECK(alloc(p, &d.src_n, n));
+  EDP_CHECK(alloc(p, &d.scores, n));
+  EDP_CHECK(alloc(p, &d.facing, n));
+  EDP_CHECK(alloc(p, &d.clipped, n));
+  EDP_CHECK(alloc(p, &d.src_lo, n));
+  EDP_CHECK(alloc(p, &d.src_hi, n));
+  d.ekey_mask = table_mask(3 * n);
+  EDP_CHECK(alloc(p, &d.ekey_table, int64_t(d.ekey_mask) + 1));
+  EDP_CHECK(alloc(p, &d.ekey_count, int64_t(d.ekey_mask) + 1));
+  EDP_CHECK(alloc(p, &d.ekey_member, 2 * (int64_t(d.ekey_mask) + 1)));
+  EDP_CHECK(alloc(p, &d.edge_slot, 3 * n));
+  EDP_CHECK(alloc(p, &d.masks, 3 * n));
+  EDP_CHECK(alloc(p, &d.edge_keys, 3 * n));
+  d.seg_mask = table_mask(S);
+  EDP_CHECK(alloc(p, &d.seg_a, S));
+  EDP_CHECK(alloc(p, &d.seg_b, S));
+  EDP_CHECK(alloc(p, &d.seg_near, S));
+  EDP_CHECK(alloc(p, &d.seg_lo, S));
+  EDP_CHECK(alloc(p, &d.seg_hi, S));
+  EDP_CHECK(alloc(p, &d.seg_slot, S));
+  EDP_CHECK(alloc(p, &d.seg_za, int64_t(d.seg_mask) + 1));
+  EDP_CHECK(alloc(p, &d.seg_zb, int64_t(d.seg_mask) + 1));
+  EDP_CHECK(alloc(p, &d.seg_table, int64_t(d.seg_mask) + 1));
+  EDP_CHECK(alloc(p, &d.seg_min, int64_t(d.seg_mask) + 1));
+  for (int k = 0; k < 2; ++k) {
+    EDP_CHECK(alloc(p, &d.fv[k], F * kMaxVertices));
+    EDP_CHECK(alloc(p, &d.fn[k], F));
+    EDP_CHECK(alloc(p, &d.fsrc[k], F));
+    EDP_CHECK(alloc(p, &d.fcur[k], F));
+  }
+  EDP_CHECK(alloc(p, &d.out_v, R * kMaxVertices));
+  EDP_CHECK(alloc(p, &d.out_n, R));
+  EDP_CHECK(alloc(p, &d.out_src, R));
+  EDP_CHECK(alloc(p, &d.out_layer, R));
+  EDP_CHECK(alloc(p, &d.counts, R));
+  EDP_CHECK(alloc(p, &d.offsets, R));
+  EDP_CHECK(alloc(p, &d.parents, R));
+  EDP_CHECK(alloc(p, &d.reps, R));
+  EDP_CHECK(alloc(p, &d.samples, R));
+  EDP_CHECK(alloc(p, &d.groups, R));
+  EDP_CHECK(alloc(p, &d.sample_slot, R));
+  d.sample_mask = table_mask(R);
+  EDP_CHECK(alloc(p, &d.sample_table, int64_t(d.sample_mask) + 1));
+  EDP_CHECK(alloc(p, &d.sample_min, int64_t(d.sample_mask) + 1));
+  EDP_CHECK(alloc(p, &d.cell_bounds, 4 * 1024));
+  EDP_CHECK(alloc(p, &d.cell_min, 1024));
+  EDP_CHECK(alloc(p, &d.cell_valid, 1024));
+  EDP_CHECK(alloc(p, &d.heavy_beams, 1024));
+  EDP_CHECK(alloc(p, &d.heavy_queries, R));
+  EDP_CHECK(alloc(p, &d.group_counts, R));
+  EDP_CHECK(alloc(p, &d.group_offsets, R));
+  EDP_CHECK(alloc(p, &d.tasks, E));
+  EDP_CHECK(alloc(p, &d.owners, E));
+  EDP_CHECK(alloc(p, &d.starts, E));
+  EDP_CHECK(alloc(p, &d.ends, E));
+  EDP_CHECK(alloc(p, &d.partners, E));
+  d.edge_hash_mask = table_mask(E);
+  EDP_CHECK(alloc(p, &d.edge_hash, int64_t(d.edge_hash_mask) + 1));
+  EDP_CHECK(alloc(p, &d.hit_depth, H));
+  EDP_CHECK(alloc(p, &d.hit_src, H));
+  EDP_CHECK(alloc(p, &d.hit_group, H));
+  EDP_CHECK(alloc(p, &d.hit_ids, H));
+  EDP_CHECK(alloc(p, &d.hit_ids_tmp, H));
+  EDP_CHECK(alloc(p, &d.hkeys, H));
+  EDP_CHECK(alloc(p, &d.hkeys_tmp, H));
+  EDP_CHECK(alloc(p, &d.bverts, E));
+  EDP_CHECK(alloc(p, &d.blayers, E));
+  EDP_CHECK(alloc(p, &d.pt_lo, E));
+  EDP_CHECK(alloc(p, &d.pt_hi, E));
+  EDP_CHECK(alloc(p, &d.mtasks, E));
+  EDP_CHECK(alloc(p, &d.tri_uv, 3 * T));
+  EDP_CHECK(alloc(p, &d.tri_world, 9 * T));
+  EDP_CHECK(alloc(p, &d.tri_src, T));
+  EDP_CHECK(alloc(p, &d.tri_layer, T));
+  EDP_CHECK(tree_alloc(p->source_tree, n));
+  EDP_CHECK(tree_alloc(p->seg_tree, S));
+  EDP_CHECK(tree_alloc(p->point_tree, E));
+  d.source_tree = p->source_tree.tree();
+  d.seg_tree = p->seg_tree.tree();
+  d.point_tree = p->point_tree.tree();
+  int64_t largest = H;
+  for (int64_t v : {p->point_tree.leaves_cap, p->seg_tree.leaves_cap, p->source_tree.leaves_cap, R})
+    largest = v > largest ? v : largest;
+  p->scratch.tiles = ceil_div(largest, kSortTile);
+  p->scratch.scan_tiles = ceil_div(R > E ? R : E, kScanTile);
+  EDP_CHECK(alloc(p, &p->scratch.hist, 256 * p->scratch.tiles));
+  EDP_CHECK(alloc(p, &p->scratch.totals, 256));
+  EDP_CHECK(alloc(p, &p->scratch.partials, p->scratch.scan_tiles));
+  return cudaSuccess;
+}
+
+// The whole extraction, recorded on `st`.  With `graph` the subdivision loop
+// becomes a conditional WHILE node of the graph being captured on `st`;
+// otherwise the host drives the loop (used by warm-up only).
+int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
+  Dev d = p->d;
+  if (!graph) {
+    d.use_handle = 0;
+    EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
+    while (true) {
+      int cond = 0;
+      EDP_TRY(cudaMemcpyAsync(&cond, d.condition, sizeof(int), cudaMemcpyDeviceToHost, st));
+      EDP_TRY(cudaStreamSynchronize(st));
+      if (!cond) break;
+      EDP_TRY(stage_step(d, st));
+    }
+    EDP_TRY(stage_rank(d, p->scratch, st));
+    EDP_TRY(stage_mesh(d, p->scratch, p->point_tree, st));
+    return EDP_OK;
+  }
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+  if (cs != cudaStreamCaptureStatusActive) return EDP_ERR_STATE;
+  cudaGraphConditionalHandle handle;
+  EDP_TRY(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+  d.use_handle = 1;
+  d.cond_handle = handle;
+  EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
+  EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
+  cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeWhile;
+  params.conditional.size = 1;
+  cudaGraphNode_t loop;
+  EDP_TRY(cudaGraphAddNode(&loop, g, deps, ndeps, &params));
+  cudaGraph_t body = params.conditional.phGraph_out[0];
+  EDP_TRY(cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies));
+  EDP_TRY(cudaStreamBeginCaptureToGraph(p->body_stream, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeRelaxed));
+  cudaError_t step = stage_step(d, p->body_stream);
+  cudaGraph_t captured = nullptr;
+  cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
+  EDP_TRY(step);
+  EDP_TRY(end);
+  EDP_TRY(stage_rank(d, p->scratch, st));
+  EDP_TRY(stage_mesh(d, p->scratch, p->point_tree, st));
+  return EDP_OK;
+}
+
+int check_inputs(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                 const double *camera, const double *settings, void *stream) {
+  if (nv < 0 || nf < 0 || nv >= (int64_t(1) << 31) || nf >= (int64_t(1) << 28))
+    return EDP_ERR_ARGUMENT;
+  if ((nv > 0 && !vertices) || (nf > 0 && !faces) || !camera || !settings || !stream)
+    return EDP_ERR_ARGUMENT;
+  return EDP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void edp_event_default_capacities(int64_t nf, edp_event_capacities *cap) {
+  int64_t n = nf > 16 ? nf : 16;
+  cap->frontier = 4 * n;
+  cap->regions = 8 * n;
+  cap->hits = 32 * n;
+  cap->vertices = 32 * n;
+  cap->triangles = 32 * n;
+  cap->rounds = 4096;
+  cap->layers = n;
+  cap->edge_vertices = 128;
+}
+
+void edp_device_default_capacities(int64_t nf, edp_device_capacities *cap) {
+  int64_t n = nf > 16 ? nf : 16;
+  cap->residual = 4 * n;
+  cap->polygons = 16 * n;
+  cap->vertices = 96 * n;
+  cap->triangles = 64 * n;
+  cap->workers = n < 4096 ? n : 4096;
+  cap->pieces_per_worker = n <= 8192 ? 512 : 2048;
+  cap->layers = 128;
+  cap->edge_vertices = 128;
+}
+
+int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                     const double *camera, const double *settings,
+                     const edp_event_capacities *cap, const edp_event_options *opt, void *stream,
+                     edp_peeler **out) {
+  if (!out) return EDP_ERR_ARGUMENT;
+  *out = nullptr;
+  int rc = check_inputs(vertices, nv, faces, nf, camera, settings, stream);
+  if (rc) return rc;
+  edp_event_capacities c;
+  if (cap)
+    c = *cap;
+  else
+    edp_event_default_capacities(nf, &c);
+  edp_event_options o{0, 1, 1, 0};
+  if (opt) o = *opt;
+  Caps caps{c.frontier, c.regions, c.hits, c.vertices, c.triangles, c.rounds, c.layers,
+            c.edge_vertices};
+  if (!caps_valid(caps)) return EDP_ERR_ARGUMENT;
+  if (o.layers < 0 || o.layers > c.layers) return EDP_ERR_ARGUMENT;
+  edp_peeler *p = new edp_peeler();
+  p->method = 0;
+  p->stream = static_cast<cudaStream_t>(stream);
+  Dev &d = p->d;
+  d.vertices = vertices;
+  d.faces = faces;
+  d.camera = camera;
+  d.settings = settings;
+  d.nv = int(nv);
+  d.n = int(nf);
+  d.cap = caps;
+  d.limit = o.layers ? o.layers : int(c.layers);
+  d.all_layers = o.layers == 0;
+  d.share_regions = o.share_regions != 0;
+  d.propagate_ranks = o.propagate_ranks != 0;
+  d.merge_regions = o.merge_regions != 0;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = allocate_event(p);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    edp_destroy(p);
+    g_last_cuda = int(e);
+    return e == cudaErrorMemoryAllocation ? EDP_ERR_MEMORY : EDP_ERR_CUDA;
+  }
+  *out = p;
+  return EDP_OK;
+}
+
+int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                      const double *camera, const double *settings,
+                      const edp_device_capacities *cap, int32_t layers, void *stream,
+                      edp_peeler **out);
+
+int edp_warmup(edp_peeler *p) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  cudaStreamCaptureStatus cs;
+  EDP_TRY(cudaStreamIsCapturing(p->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return EDP_ERR_STATE;
+  int rc = enqueue_events(p, p->stream, false);
+  if (rc) return rc;
+  EDP_TRY(cudaStreamSynchronize(p->stream));
+  p->warmed = true;
+  return EDP_OK;
+}
+
+int edp_enqueue(edp_peeler *p, void *stream) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  if (!p->warmed || static_cast<cudaStream_t>(stream) != p->stream) return EDP_ERR_STATE;
+  cudaStreamCaptureStatus cs;
+  EDP_TRY(cudaStreamIsCapturing(p->stream, &cs));
+  if (cs != cudaStreamCaptureStatusActive) return EDP_ERR_STATE;
+  return enqueue_events(p, p->stream, true);
+}
+
+int edp_capture(edp_peeler *p) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  if (p->exec) return EDP_OK;
+  if (!p->warmed) {
+    int rc = edp_warmup(p);
+    if (rc) return rc;
+  }
+  EDP_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_events(p, p->stream, true);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  EDP_TRY(e);
+  p->graph = g;
+  EDP_TRY(cudaGraphInstantiate(&p->exec, g, 0));
+  return EDP_OK;
+}
+
+int edp_run(edp_peeler *p) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  if (!p->exec) {
+    int rc = edp_capture(p);
+    if (rc) return rc;
+  }
+  EDP_TRY(cudaGraphLaunch(p->exec, p->stream));
+  return EDP_OK;
+}
+
+int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  EDP_TRY(cudaStreamSynchronize(p->stream));
+  if (status)
+    EDP_TRY(cudaMemcpy(status, p->d.status, sizeof(int32_t) * kStatusSlots, cudaMemcpyDeviceToHost));
+  if (metrics)
+    EDP_TRY(cudaMemcpy(metrics, p->d.metrics, sizeof(int64_t) * kMetrics, cudaMemcpyDeviceToHost));
+  return EDP_OK;
+}
+
+int edp_get_outputs(edp_peeler *p, edp_outputs *o) {
+  if (!p || !o) return EDP_ERR_ARGUMENT;
+  const Dev &d = p->d;
+  o->status = d.status;
+  o->metrics = reinterpret_cast<int64_t *>(d.metrics);
+  o->output_vertices = reinterpret_cast<double *>(d.out_v);
+  o->output_sizes = d.out_n;
+  o->output_sources = d.out_src;
+  o->output_layers = d.out_layer;
+  o->triangles_uv = reinterpret_cast<double *>(d.tri_uv);
+  o->triangles_world = d.tri_world;
+  o->triangle_sources = d.tri_src;
+  o->triangle_layers = d.tri_layer;
+  o->canonical = d.canonical;
+  o->regions = d.cap.regions;
+  o->triangles = d.cap.triangles;
+  o->vertices = d.cap.vertices;
+  return EDP_OK;
+}
+
+void edp_destroy(edp_peeler *p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  tree_free(p->source_tree);
+  tree_free(p->seg_tree);
+  tree_free(p->point_tree);
+  for (void *a : p->allocations) cudaFree(a);
+  if (p->body_stream) cudaStreamDestroy(p->body_stream);
+  delete p;
+}
+
+const char *edp_status_string(int code) {
+  switch (code) {
+    case EDP_OK: return "ok";
+    case EDP_ERR_ARGUMENT: return "invalid argument";
+    case EDP_ERR_STATE: return "invalid call order or capture state";
+    case EDP_ERR_CUDA: return "CUDA runtime error";
+    case EDP_ERR_MEMORY: return "device memory allocation failed";
+    default: return "unknown status";
+  }
+}
+
+int edp_last_cuda_error(void) { return g_last_cuda; }
+int edp_abi_version(void) { return 1; }
+
+}  // extern "C"

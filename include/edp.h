@@ -1,0 +1,140 @@
+/*
+ * edp.h - C ABI of libedp_b200, the B200 analytic depth peeler.
+ *
+ * Plain pointers and sizes only.  All geometry pointers are CUDA device
+ * pointers owned by the caller; the workspace owns every pool and output
+ * buffer and must outlive any CUDA graph that replays it.  Each entry point
+ * returns an edp_status code (0 on success); device-side failures are not
+ * return codes but sticky bits in status[9], read with edp_read_status.
+ *
+ * The reference binds this path through Python (Warp arrays, not an FFI); the
+ * entry points below replace its call surface one to one:
+ *
+ *   edp_event_create   warp_peel/events.py:43-138   EventPeeler.__init__
+ *   edp_device_create  warp_peel/solver.py:103-212  DevicePeeler.__init__
+ *   edp_warmup         warp_peel/events.py:782-796  EventPeeler.warmup
+ *   edp_enqueue        warp_peel/events.py:798-806  EventPeeler.enqueue
+ *   edp_capture        warp_peel/solver.py:471-480  DevicePeeler.capture
+ *   edp_run            warp_peel/solver.py:482-486  DevicePeeler.run
+ *   edp_read_status    warp_peel/events.py:808-845  EventPeeler.read_status
+ *                      (status[16] and metrics[19] arrays; solver.py:154-156,
+ *                      events.py:103)
+ *   edp_get_outputs    the device attributes read by warp_peel/io.py:51-72
+ *                      and tests/gpu/test_peeler.py:24-34
+ *   edp_destroy        workspace release (Warp frees arrays on collection)
+ */
+#ifndef EDP_H
+#define EDP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct edp_peeler edp_peeler;
+
+enum edp_status {
+  EDP_OK = 0,
+  EDP_ERR_ARGUMENT = 1, /* invalid argument (the reference raises ValueError) */
+  EDP_ERR_STATE = 2,    /* capture misuse (the reference raises RuntimeError) */
+  EDP_ERR_CUDA = 3,     /* a CUDA runtime call failed; see edp_last_cuda_error */
+  EDP_ERR_MEMORY = 4    /* pool allocation failed */
+};
+
+/* Status slots and error bits (warp_peel/kernels.py:17-21, README.md:175-184). */
+enum {
+  EDP_STATUS_SLOTS = 16,
+  EDP_METRICS = 19,
+  EDP_ERR_BIT_POLYGON = 1,
+  EDP_ERR_BIT_WORKER = 2,
+  EDP_ERR_BIT_RESIDUAL = 4,
+  EDP_ERR_BIT_OUTPUT = 8,
+  EDP_ERR_BIT_VERTICES = 16,
+  EDP_ERR_BIT_TRIANGLES = 32,
+  EDP_ERR_BIT_LAYERS = 64,
+  EDP_ERR_BIT_EDGE_NODING = 128,
+  EDP_ERR_BIT_INPUT = 256,
+  EDP_ERR_BIT_HITS = 1024,
+  EDP_ERR_BIT_ROUNDS = 2048
+};
+
+/* warp_peel/events.py:19-33 (EventCapacities). */
+typedef struct edp_event_capacities {
+  int64_t frontier, regions, hits, vertices, triangles, rounds, layers, edge_vertices;
+} edp_event_capacities;
+
+/* warp_peel/events.py:43-55 (layers, share_regions, propagate_ranks, merge_regions). */
+typedef struct edp_event_options {
+  int32_t layers; /* 0 = all layers */
+  int32_t share_regions, propagate_ranks, merge_regions;
+} edp_event_options;
+
+/* warp_peel/solver.py:10-31 (Capacities). */
+typedef struct edp_device_capacities {
+  int64_t residual, polygons, vertices, triangles, workers, pieces_per_worker, layers,
+      edge_vertices;
+} edp_device_capacities;
+
+/* Device pointers of the workspace's buffers.  Counts live in status:
+ * status[2] polygons, status[3] triangles, status[6] boundary vertices. */
+typedef struct edp_outputs {
+  int32_t *status;          /* [16] */
+  int64_t *metrics;         /* [19] */
+  double *output_vertices;  /* [regions][32][2] polygon vertices */
+  int32_t *output_sizes;    /* [regions] vertex counts (0 = suppressed) */
+  int32_t *output_sources;  /* [regions] dense source (face) index */
+  int32_t *output_layers;   /* [regions] zero-based depth rank */
+  double *triangles_uv;     /* [triangles][3][2] normalised window coordinates */
+  double *triangles_world;  /* [triangles][3][3] world coordinates */
+  int32_t *triangle_sources;
+  int32_t *triangle_layers;
+  int32_t *canonical;       /* [nv] welded vertex ids */
+  int64_t regions, triangles, vertices;
+} edp_outputs;
+
+/* Create an EventPeeler workspace (contour subdivision + shared ray ranks).
+ * vertices: double[nv][3]; faces: int32[nf][3]; camera: double[4][4] row-major
+ * affine world-to-camera; settings: double[6] = xmin, ymin, xmax, ymax,
+ * perspective (0/1), near.  stream: the workspace's cudaStream_t.  cap and opt
+ * may be NULL for the reference defaults (EventCapacities.for_mesh). */
+int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                     const double *camera, const double *settings,
+                     const edp_event_capacities *cap, const edp_event_options *opt, void *stream,
+                     edp_peeler **out);
+
+/* Default capacities for a mesh of nf faces (events.py:30-33 / solver.py:21-31). */
+void edp_event_default_capacities(int64_t nf, edp_event_capacities *cap);
+void edp_device_default_capacities(int64_t nf, edp_device_capacities *cap);
+
+/* Create a DevicePeeler workspace (iterative per-layer clipping). */
+int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                      const double *camera, const double *settings,
+                      const edp_device_capacities *cap, int32_t layers, void *stream,
+                      edp_peeler **out);
+
+/* One eager extraction with host-driven loop control, then synchronise. */
+int edp_warmup(edp_peeler *p);
+/* Record the whole extraction into the capture in progress on `stream`, which
+ * must be the workspace stream.  No host reads or allocations are recorded. */
+int edp_enqueue(edp_peeler *p, void *stream);
+/* Capture and instantiate the workspace's own graph (idempotent). */
+int edp_capture(edp_peeler *p);
+/* Asynchronous replay of the captured graph on the workspace stream. */
+int edp_run(edp_peeler *p);
+/* Synchronise the workspace stream and copy status[16] / metrics[19] out
+ * (either may be NULL). */
+int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics);
+int edp_get_outputs(edp_peeler *p, edp_outputs *out);
+void edp_destroy(edp_peeler *p);
+
+/* Human-readable edp_status; the last CUDA error code of this thread. */
+const char *edp_status_string(int code);
+int edp_last_cuda_error(void);
+int edp_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EDP_H */
