@@ -178,5 +178,10 @@ cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree
 cudaError_t stage_step(const Dev &d, cudaStream_t st);
 cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st);
 cudaError_t stage_mesh(const Dev &d, SortScratch &s, TreeBuffers &point_tree, cudaStream_t st);
+// The two halves of stage_mesh: boundary vertices and point hierarchy, then
+// the noding / emission / lifting kernel.
+cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
+                             cudaStream_t st);
+cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st);
 
 }  // namespace edp

@@ -157,16 +157,26 @@ unsigned blocks(int64_t n) {
 
 }  // namespace
 
-cudaError_t stage_mesh(const Dev &d, SortScratch &s, TreeBuffers &point_tree, cudaStream_t st) {
-  const int64_t R = d.cap.regions, E = d.cap.vertices;
+cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
+                             cudaStream_t st) {
+  const int64_t R = d.cap.regions;
   k_mesh_counts<<<blocks(R), kBlock, 0, st>>>(d);
   EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
   k_mesh_check<<<1, 1, 0, st>>>(d);
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kLiveVertices, 0, true, s, st));
-  int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
-  k_mesh_edges<<<blocks(E), kBlock, 0, st>>>(d, cap);
   return cudaGetLastError();
+}
+
+cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st) {
+  int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
+  k_mesh_edges<<<blocks(d.cap.vertices), kBlock, 0, st>>>(d, cap);
+  return cudaGetLastError();
+}
+
+cudaError_t stage_mesh(const Dev &d, SortScratch &s, TreeBuffers &point_tree, cudaStream_t st) {
+  EDP_CHECK(stage_mesh_index(d, s, point_tree, st));
+  return stage_mesh_emit(d, st);
 }
 
 }  // namespace edp

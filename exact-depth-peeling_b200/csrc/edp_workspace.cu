@@ -9,6 +9,12 @@
 
 using namespace edp;
 
+namespace {
+// start, after preparation, after the subdivision loop, after ranking,
+// before and after the noding/emission kernel.
+constexpr int kProfileMarks = 6;
+}  // namespace
+
 struct edp_peeler {
   int method = 0;  // 0 = EventPeeler, 1 = DevicePeeler
   Dev d{};
@@ -21,11 +27,32 @@ struct edp_peeler {
   cudaGraphExec_t exec = nullptr;
   bool warmed = false;
   int device = 0;
+  // Optional stage markers recorded as event nodes inside the captured graph.
+  bool profile = false;
+  cudaEvent_t marks[kProfileMarks] = {};
+  // Kernel nodes of the last capture: outside the subdivision loop, and in
+  // one iteration of its body.
+  int64_t kernels_outside = 0, kernels_per_round = 0;
 };
 
 namespace {
 
 thread_local int g_last_cuda = 0;
+
+cudaError_t count_kernels(cudaGraph_t g, int64_t &count) {
+  size_t n = 0;
+  cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+  if (e != cudaSuccess) return e;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
+  count = 0;
+  for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
+    cudaGraphNodeType t;
+    e = cudaGraphNodeGetType(nodes[i], &t);
+    count += t == cudaGraphNodeTypeKernel;
+  }
+  return e;
+}
 
 int cuda_fail(cudaError_t e) {
   g_last_cuda = int(e);
@@ -195,7 +222,13 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
   d.use_handle = 1;
   d.cond_handle = handle;
+  auto mark = [&](int k) -> cudaError_t {
+    return p->profile ? cudaEventRecordWithFlags(p->marks[k], st, cudaEventRecordExternal)
+                      : cudaSuccess;
+  };
+  EDP_TRY(mark(0));
   EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
+  EDP_TRY(mark(1));
   EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
   cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
@@ -214,8 +247,14 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
   EDP_TRY(step);
   EDP_TRY(end);
+  EDP_TRY(count_kernels(body, p->kernels_per_round));
+  EDP_TRY(mark(2));
   EDP_TRY(stage_rank(d, p->scratch, st));
-  EDP_TRY(stage_mesh(d, p->scratch, p->point_tree, st));
+  EDP_TRY(mark(3));
+  EDP_TRY(stage_mesh_index(d, p->scratch, p->point_tree, st));
+  EDP_TRY(mark(4));
+  EDP_TRY(stage_mesh_emit(d, st));
+  EDP_TRY(mark(5));
   return EDP_OK;
 }
 
@@ -347,6 +386,7 @@ int edp_capture(edp_peeler *p) {
   }
   EDP_TRY(e);
   p->graph = g;
+  EDP_TRY(count_kernels(g, p->kernels_outside));
   EDP_TRY(cudaGraphInstantiate(&p->exec, g, 0));
   return EDP_OK;
 }
@@ -400,6 +440,8 @@ void edp_destroy(edp_peeler *p) {
   tree_free(p->point_tree);
   for (void *a : p->allocations) cudaFree(a);
   if (p->body_stream) cudaStreamDestroy(p->body_stream);
+  for (auto &e : p->marks)
+    if (e) cudaEventDestroy(e);
   delete p;
 }
 
@@ -412,6 +454,32 @@ const char *edp_status_string(int code) {
     case EDP_ERR_MEMORY: return "device memory allocation failed";
     default: return "unknown status";
   }
+}
+
+int edp_profile(edp_peeler *p, int32_t enable) {
+  if (!p) return EDP_ERR_ARGUMENT;
+  if (p->exec) return EDP_ERR_STATE;  // markers are fixed at capture time
+  if (enable && !p->marks[0])
+    for (auto &e : p->marks) EDP_TRY(cudaEventCreate(&e));
+  p->profile = enable != 0;
+  return EDP_OK;
+}
+
+int edp_profile_read(edp_peeler *p, float *ms, int32_t count) {
+  if (!p || !ms || count < kProfileMarks - 1) return EDP_ERR_ARGUMENT;
+  if (!p->profile || !p->exec) return EDP_ERR_STATE;
+  EDP_TRY(cudaStreamSynchronize(p->stream));
+  for (int k = 0; k + 1 < kProfileMarks; ++k)
+    EDP_TRY(cudaEventElapsedTime(&ms[k], p->marks[k], p->marks[k + 1]));
+  return EDP_OK;
+}
+
+int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round) {
+  if (!p || !outside_loop || !per_round) return EDP_ERR_ARGUMENT;
+  if (!p->exec) return EDP_ERR_STATE;
+  *outside_loop = p->kernels_outside;
+  *per_round = p->kernels_per_round;
+  return EDP_OK;
 }
 
 int edp_last_cuda_error(void) { return g_last_cuda; }

@@ -1,0 +1,183 @@
+"""Seeded synthetic scenes for the benchmark configurations.
+
+Every generator returns host numpy arrays ``(vertices float64 [V,3], faces
+int32 [N,3], camera float64 [4,4], settings float64 [6])`` with shared
+(welded) vertices, so the peeler sees mesh connectivity.  The shapes, sizes
+and value distributions follow the benchmark's configuration text; no public
+dataset is involved.
+"""
+
+import math
+
+import numpy as np
+
+
+def _ortho_down_z(vertices, margin=0.05):
+    """Orthographic view along world -z (camera = diag(1, 1, -1)); the window is
+    the xy bounding box grown by ``margin`` on each side."""
+    camera = np.diag([1.0, 1.0, -1.0, 1.0])
+    lo, hi = vertices[:, :2].min(0), vertices[:, :2].max(0)
+    pad = margin * (hi - lo)
+    settings = np.array([lo[0] - pad[0], lo[1] - pad[1], hi[0] + pad[0], hi[1] + pad[1], 0.0,
+                         0.01])
+    return camera, settings
+
+
+def _pinhole(eye, target, fov_degrees=60.0, near=0.01):
+    """Pinhole camera at ``eye`` looking at ``target``; camera z is depth
+    (positive in front), the window is the normalised image plane +-tan(fov/2)."""
+    eye, target = np.asarray(eye, float), np.asarray(target, float)
+    forward = target - eye
+    forward /= np.linalg.norm(forward)
+    up = np.array([0.0, 1.0, 0.0]) if abs(forward[1]) < 0.9 else np.array([1.0, 0.0, 0.0])
+    right = np.cross(up, forward)
+    right /= np.linalg.norm(right)
+    true_up = np.cross(forward, right)
+    rotation = np.stack([right, true_up, forward])
+    camera = np.eye(4)
+    camera[:3, :3] = rotation
+    camera[:3, 3] = -rotation @ eye
+    h = math.tan(math.radians(fov_degrees) / 2)
+    settings = np.array([-h, -h, h, h, 1.0, near])
+    return camera, settings
+
+
+def icosphere(subdivisions):
+    """Unit icosphere: 20 * 4**subdivisions faces, outward (ccw) winding."""
+    t = (1 + 5 ** 0.5) / 2
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t),
+             (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+             (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+             (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(v, float) / np.linalg.norm(v) for v in verts]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nxt = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nxt += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nxt
+    return np.array(verts), np.array(faces, dtype=np.int32)
+
+
+def nested_icospheres(seed=0):
+    """Two nested noisy icospheres (2 x 1,280 faces), orthographic view down -z.
+
+    Outer radii lie in [0.85, 1.15], the inner copy's in [0.425, 0.575]: the
+    shells cannot intersect.  About four layers."""
+    v, f = icosphere(3)
+    rng0, rng1 = np.random.default_rng(seed), np.random.default_rng(seed + 1)
+    outer = v * (1 + rng0.uniform(-0.15, 0.15, size=(len(v), 1)))
+    inner = 0.5 * v * (1 + rng1.uniform(-0.15, 0.15, size=(len(v), 1)))
+    vertices = np.concatenate([outer, inner])
+    faces = np.concatenate([f, f + len(v)]).astype(np.int32)
+    camera, settings = _ortho_down_z(vertices)
+    return vertices, faces, camera, settings
+
+
+def torus_knot(t, p=3, q=7):
+    r = 2 + np.cos(q * t)
+    return np.stack([r * np.cos(p * t), r * np.sin(p * t), np.sin(q * t)], axis=-1)
+
+
+def knot_tube(rings=256, segments=128, radius=0.3, noise=0.02, seed=2):
+    """Tube swept along a (3,7) torus knot: rings x segments quads split into
+    2 * rings * segments triangles (65,536 by default), radius noise N(0, noise)
+    per vertex, pinhole camera with a 60 degree field of view at 3x the
+    bounding radius on +z looking at the centroid.  The radius 0.3 keeps the
+    knot strands 1.26 tube diameters apart (``knot_clearance``), so the tube
+    has no self-intersections to resolve."""
+    rng = np.random.default_rng(seed)
+    t = np.linspace(0, 2 * np.pi, rings, endpoint=False)
+    dt = 1e-4
+    center = torus_knot(t)
+    tangent = torus_knot(t + dt) - torus_knot(t - dt)
+    tangent /= np.linalg.norm(tangent, axis=1, keepdims=True)
+    # Rotation-minimising frame by parallel transport, closed with a twist fix.
+    normal = np.zeros_like(center)
+    n0 = np.cross(tangent[0], [0.0, 0.0, 1.0])
+    normal[0] = n0 / np.linalg.norm(n0)
+    for i in range(1, rings):
+        n = normal[i - 1] - np.dot(normal[i - 1], tangent[i]) * tangent[i]
+        normal[i] = n / np.linalg.norm(n)
+    binormal = np.cross(tangent, normal)
+    last = normal[-1] - np.dot(normal[-1], tangent[0]) * tangent[0]
+    last /= np.linalg.norm(last)
+    twist = math.atan2(np.dot(np.cross(last, normal[0]), tangent[0]), np.dot(last, normal[0]))
+    theta = np.linspace(0, 2 * np.pi, segments, endpoint=False)
+    angle = theta[None, :] + twist * (np.arange(rings) / rings)[:, None]
+    r = radius * (1 + rng.normal(0.0, noise, size=(rings, segments)))
+    vertices = (center[:, None, :]
+                + r[..., None] * (np.cos(angle)[..., None] * normal[:, None, :]
+                                  + np.sin(angle)[..., None] * binormal[:, None, :]))
+    vertices = vertices.reshape(-1, 3)
+    i = np.arange(rings)[:, None]
+    j = np.arange(segments)[None, :]
+    a = i * segments + j
+    b = ((i + 1) % rings) * segments + j
+    c = ((i + 1) % rings) * segments + (j + 1) % segments
+    d = i * segments + (j + 1) % segments
+    faces = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3),
+                            np.stack([a, c, d], -1).reshape(-1, 3)]).astype(np.int32)
+    centroid = vertices.mean(0)
+    bound = np.linalg.norm(vertices - centroid, axis=1).max()
+    camera, settings = _pinhole(centroid + np.array([0.0, 0.0, 3 * bound]), centroid,
+                                near=0.01 * bound)
+    return vertices, faces, camera, settings
+
+
+def knot_clearance(rings=2048, radius=0.3, noise=0.02):
+    """Smallest centreline distance between knot points more than one tube
+    diameter apart along the curve, divided by the largest tube diameter
+    (4 sigma noise); > 1 means the swept tube cannot self-intersect."""
+    t = np.linspace(0, 2 * np.pi, rings, endpoint=False)
+    c = torus_knot(t)
+    step = np.linalg.norm(np.diff(c, axis=0), axis=1).mean()
+    diameter = 2 * radius * (1 + 4 * noise)
+    separation = int(np.ceil(3 * diameter / step))
+    best = np.inf
+    for k in range(rings):
+        d = np.linalg.norm(c - c[k], axis=1)
+        idx = np.arange(rings)
+        gap = np.minimum(np.abs(idx - k), rings - np.abs(idx - k))
+        far = gap > separation
+        best = min(best, d[far].min())
+    return best / diameter
+
+
+def stress_stack(n=65536, jitter=1e-9, seed=3):
+    """n congruent triangles at z = i * 1e-3 with per-vertex xy jitter
+    U(-jitter, jitter), orthographic view (n layers)."""
+    rng = np.random.default_rng(seed)
+    base = np.array([[-0.75, -0.75], [0.75, -0.75], [0.0, 0.75]])
+    xy = base[None] + rng.uniform(-jitter, jitter, size=(n, 3, 2)) if jitter else np.repeat(
+        base[None], n, 0)
+    z = (np.arange(n) * 1e-3)[:, None, None] * np.ones((n, 3, 1))
+    vertices = np.concatenate([xy, z], axis=2).reshape(-1, 3)
+    faces = np.arange(3 * n, dtype=np.int32).reshape(-1, 3)
+    camera = np.diag([1.0, 1.0, -1.0, 1.0])
+    settings = np.array([-1.0, -1.0, 1.0, 1.0, 0.0, 0.01])
+    return vertices, faces, camera, settings
+
+
+CONFIGS = {
+    "icospheres-2560": nested_icospheres,
+    "knot-65536": knot_tube,
+    "stack-65536": lambda: stress_stack(65536, 0.0),
+}
+
+
+def to_device(arrays, device="cuda:0"):
+    import torch
+
+    return [torch.as_tensor(np.ascontiguousarray(a), device=device) for a in arrays]

@@ -128,6 +128,18 @@ int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics);
 int edp_get_outputs(edp_peeler *p, edp_outputs *out);
 void edp_destroy(edp_peeler *p);
 
+/* Stage timing: with enable != 0 before the first capture, CUDA event nodes
+ * are recorded between stages inside the graph.  edp_profile_read returns the
+ * milliseconds of the last replay's stages: [0] preparation, [1] subdivision
+ * loop, [2] ranking, [3] boundary vertices + point hierarchy, [4] the noding /
+ * emission / lifting kernel (count >= 5).  Project-specific: the reference
+ * times separately captured stage graphs instead (scripts/profile_events.py). */
+int edp_profile(edp_peeler *p, int32_t enable);
+int edp_profile_read(edp_peeler *p, float *ms, int32_t count);
+/* Kernel nodes of the captured graph: outside the subdivision loop, and per
+ * loop iteration (a replay launches outside + per_round * rounds kernels). */
+int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
+
 /* Human-readable edp_status; the last CUDA error code of this thread. */
 const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
