@@ -178,7 +178,6 @@ def run_ours(args, rank, world, local_rank):
     arrays = scenes.to_device(host, device)
     p = EventPeeler(*arrays)
     lib = _lib.load()
-    _lib.check(lib.edp_profile(p._ws.handle, 1), "profile")
     p.capture()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
     for _ in range(args.warmup):
@@ -187,11 +186,8 @@ def run_ours(args, rank, world, local_rank):
     stream = p.stream
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stages = []
-    import ctypes
     import numpy as np
 
-    stage_ms = np.zeros(5, dtype=np.float32)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -202,8 +198,6 @@ def run_ours(args, rank, world, local_rank):
                 starts[k].record(stream)
             p.run()
             ends[k].record(stream)
-            _lib.check(lib.edp_profile_read(p._ws.handle, stage_ms.ctypes.data, 5), "profile")
-            stages.append(stage_ms.copy())
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -214,7 +208,26 @@ def run_ours(args, rank, world, local_rank):
     total = float(launches_ms.item())
     ms_per_mesh = total / (args.steps * world)
     check = p.read_status()
-    stage_mean = np.mean(np.stack(stages), axis=0)
+    # Stage timing, as the reference profiles (scripts/profile_events.py): each
+    # stage replayed alone from its own captured graph, CUDA events on the
+    # workspace stream, L2 flushed before each replay.
+    stage_ms = {}
+    for stage, name in ((0, "prepare"), (1, "mesh_index"), (2, "mesh_emit")):
+        times = []
+        for k in range(max(3, args.steps)):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            _lib.check(lib.edp_run_stage(p._ws.handle, stage), "stage")
+            b.record(stream)
+            b.synchronize()
+            if k > 0:
+                times.append(a.elapsed_time(b))
+        stage_ms[name] = statistics.median(times)
+    p.run()  # restore the full extraction's state after the stage replays
+    p.read_status()
+    stage_ms["subdivision_and_rank"] = total / args.steps - sum(stage_ms.values())
 
     # End to end through the public API: pinned host inputs uploaded each step,
     # the extraction replayed, then status and every triangle read back.
@@ -247,13 +260,11 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     peak, peak_kind = hbm_peak()
-    names = ["prepare", "subdivision_loop", "rank", "mesh_index", "mesh_emit"]
-    dominant = int(np.argmax(stage_mean))
     mesh_bytes = algorithmic_bytes(len(vertices), len(faces), check["triangles"])
     # Noding / emission kernel: every output triangle written once (128 B), each
     # boundary vertex read once (16 B) and each polygon's header (32 B).
     emit_bytes = 128 * check["triangles"] + 16 * check["boundary_vertices"] + 32 * check["polygons"]
-    emit_ms = float(stage_mean[4])
+    emit_ms = float(stage_ms["mesh_emit"])
     roofline = {
         "bound": "hbm", "kernel": "k_mesh_edges (noding, fan emission, world lift)",
         "achieved": emit_bytes / (emit_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -273,8 +284,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h_bytes)},
         "gpu_launches": None, "clocks": clocks.summary(),
-        "stages_ms": dict(zip(names, map(float, stage_mean))),
-        "dominant_stage": names[dominant],
+        "stages_ms": stage_ms,
         "output": {k: check[k] for k in ("polygons", "triangles", "layers", "boundary_vertices")},
     }
     outside = np.zeros(2, dtype=np.int64)

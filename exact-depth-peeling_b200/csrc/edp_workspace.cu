@@ -10,9 +10,10 @@
 using namespace edp;
 
 namespace {
-// start, after preparation, after the subdivision loop, after ranking,
-// before and after the noding/emission kernel.
-constexpr int kProfileMarks = 6;
+// Stages that can be replayed alone after a full extraction, each from its own
+// captured graph: preparation, boundary vertices + point hierarchy, and the
+// noding / emission / lifting kernel.
+constexpr int kStages = 3;
 }  // namespace
 
 struct edp_peeler {
@@ -27,9 +28,7 @@ struct edp_peeler {
   cudaGraphExec_t exec = nullptr;
   bool warmed = false;
   int device = 0;
-  // Optional stage markers recorded as event nodes inside the captured graph.
-  bool profile = false;
-  cudaEvent_t marks[kProfileMarks] = {};
+  cudaGraphExec_t stage_exec[kStages] = {};
   // Kernel nodes of the last capture: outside the subdivision loop, and in
   // one iteration of its body.
   int64_t kernels_outside = 0, kernels_per_round = 0;
@@ -222,13 +221,7 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
   d.use_handle = 1;
   d.cond_handle = handle;
-  auto mark = [&](int k) -> cudaError_t {
-    return p->profile ? cudaEventRecordWithFlags(p->marks[k], st, cudaEventRecordExternal)
-                      : cudaSuccess;
-  };
-  EDP_TRY(mark(0));
   EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
-  EDP_TRY(mark(1));
   EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
   cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
@@ -248,13 +241,9 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(step);
   EDP_TRY(end);
   EDP_TRY(count_kernels(body, p->kernels_per_round));
-  EDP_TRY(mark(2));
   EDP_TRY(stage_rank(d, p->scratch, st));
-  EDP_TRY(mark(3));
   EDP_TRY(stage_mesh_index(d, p->scratch, p->point_tree, st));
-  EDP_TRY(mark(4));
   EDP_TRY(stage_mesh_emit(d, st));
-  EDP_TRY(mark(5));
   return EDP_OK;
 }
 
@@ -440,8 +429,8 @@ void edp_destroy(edp_peeler *p) {
   tree_free(p->point_tree);
   for (void *a : p->allocations) cudaFree(a);
   if (p->body_stream) cudaStreamDestroy(p->body_stream);
-  for (auto &e : p->marks)
-    if (e) cudaEventDestroy(e);
+  for (auto &e : p->stage_exec)
+    if (e) cudaGraphExecDestroy(e);
   delete p;
 }
 
@@ -456,21 +445,31 @@ const char *edp_status_string(int code) {
   }
 }
 
-int edp_profile(edp_peeler *p, int32_t enable) {
-  if (!p) return EDP_ERR_ARGUMENT;
-  if (p->exec) return EDP_ERR_STATE;  // markers are fixed at capture time
-  if (enable && !p->marks[0])
-    for (auto &e : p->marks) EDP_TRY(cudaEventCreate(&e));
-  p->profile = enable != 0;
-  return EDP_OK;
-}
-
-int edp_profile_read(edp_peeler *p, float *ms, int32_t count) {
-  if (!p || !ms || count < kProfileMarks - 1) return EDP_ERR_ARGUMENT;
-  if (!p->profile || !p->exec) return EDP_ERR_STATE;
-  EDP_TRY(cudaStreamSynchronize(p->stream));
-  for (int k = 0; k + 1 < kProfileMarks; ++k)
-    EDP_TRY(cudaEventElapsedTime(&ms[k], p->marks[k], p->marks[k + 1]));
+int edp_run_stage(edp_peeler *p, int32_t stage) {
+  if (!p || stage < 0 || stage >= kStages) return EDP_ERR_ARGUMENT;
+  if (!p->exec) return EDP_ERR_STATE;  // stages replay the state of a full run
+  if (!p->stage_exec[stage]) {
+    Dev d = p->d;
+    d.use_handle = 0;
+    EDP_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    if (stage == 0) {
+      e = stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, p->stream);
+    } else if (stage == 1) {
+      e = stage_mesh_index(d, p->scratch, p->point_tree, p->stream);
+    } else {
+      e = cudaMemsetAsync(d.status + kTriangles, 0, sizeof(int), p->stream);
+      if (e == cudaSuccess) e = stage_mesh_emit(d, p->stream);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t end = cudaStreamEndCapture(p->stream, &g);
+    EDP_TRY(e);
+    EDP_TRY(end);
+    e = cudaGraphInstantiate(&p->stage_exec[stage], g, 0);
+    cudaGraphDestroy(g);
+    EDP_TRY(e);
+  }
+  EDP_TRY(cudaGraphLaunch(p->stage_exec[stage], p->stream));
   return EDP_OK;
 }
 

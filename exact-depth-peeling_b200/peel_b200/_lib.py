@@ -43,8 +43,7 @@ EXPORTS = (
     "edp_event_create", "edp_device_create", "edp_event_default_capacities",
     "edp_device_default_capacities", "edp_warmup", "edp_enqueue", "edp_capture", "edp_run",
     "edp_read_status", "edp_get_outputs", "edp_destroy", "edp_status_string",
-    "edp_last_cuda_error", "edp_abi_version", "edp_profile", "edp_profile_read",
-    "edp_graph_kernels",
+    "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
 )
 
 _lib = None
@@ -78,8 +77,7 @@ def load():
     lib.edp_enqueue.argtypes = [P, P]
     lib.edp_read_status.argtypes = [P, P, P]
     lib.edp_get_outputs.argtypes = [P, ctypes.POINTER(OutputsC)]
-    lib.edp_profile.argtypes = [P, I32]
-    lib.edp_profile_read.argtypes = [P, P, I32]
+    lib.edp_run_stage.argtypes = [P, I32]
     lib.edp_graph_kernels.argtypes = [P, P, P]
     lib.edp_destroy.argtypes = [P]
     lib.edp_destroy.restype = None

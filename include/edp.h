@@ -128,14 +128,13 @@ int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics);
 int edp_get_outputs(edp_peeler *p, edp_outputs *out);
 void edp_destroy(edp_peeler *p);
 
-/* Stage timing: with enable != 0 before the first capture, CUDA event nodes
- * are recorded between stages inside the graph.  edp_profile_read returns the
- * milliseconds of the last replay's stages: [0] preparation, [1] subdivision
- * loop, [2] ranking, [3] boundary vertices + point hierarchy, [4] the noding /
- * emission / lifting kernel (count >= 5).  Project-specific: the reference
- * times separately captured stage graphs instead (scripts/profile_events.py). */
-int edp_profile(edp_peeler *p, int32_t enable);
-int edp_profile_read(edp_peeler *p, float *ms, int32_t count);
+/* Replay one stage alone, from its own captured graph, on the workspace
+ * stream, after at least one full run: 0 preparation, 1 boundary vertices +
+ * point hierarchy, 2 the noding / emission / lifting kernel.  Used to time
+ * stages with CUDA events, as the reference's profiler times separately
+ * captured stage graphs (scripts/profile_events.py:35-98).  Replaying stage 0
+ * resets the counters, so run the full graph again before reading outputs. */
+int edp_run_stage(edp_peeler *p, int32_t stage);
 /* Kernel nodes of the captured graph: outside the subdivision loop, and per
  * loop iteration (a replay launches outside + per_round * rounds kernels). */
 int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
