@@ -29,6 +29,7 @@ struct edp_peeler {
   bool warmed = false;
   int device = 0;
   cudaGraphExec_t stage_exec[kStages] = {};
+  cudaGraph_t body_graph = nullptr;  // loop body of the last own capture (owned by graph)
   // Kernel nodes of the last capture: outside the subdivision loop, and in
   // one iteration of its body.
   int64_t kernels_outside = 0, kernels_per_round = 0;
@@ -37,6 +38,7 @@ struct edp_peeler {
 namespace {
 
 thread_local int g_last_cuda = 0;
+thread_local const char *g_last_site = "";
 
 cudaError_t count_kernels(cudaGraph_t g, int64_t &count) {
   size_t n = 0;
@@ -53,15 +55,18 @@ cudaError_t count_kernels(cudaGraph_t g, int64_t &count) {
   return e;
 }
 
-int cuda_fail(cudaError_t e) {
+int cuda_fail(cudaError_t e, const char *site) {
   g_last_cuda = int(e);
+  g_last_site = site;
   return EDP_ERR_CUDA;
 }
 
-#define EDP_TRY(call)                                   \
-  do {                                                  \
-    cudaError_t e__ = (call);                           \
-    if (e__ != cudaSuccess) return cuda_fail(e__);      \
+#define EDP_STR2(x) #x
+#define EDP_STR(x) EDP_STR2(x)
+#define EDP_TRY(call)                                                              \
+  do {                                                                             \
+    cudaError_t e__ = (call);                                                      \
+    if (e__ != cudaSuccess) return cuda_fail(e__, __FILE__ ":" EDP_STR(__LINE__)); \
   } while (0)
 
 template <class T>
@@ -240,7 +245,7 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
   EDP_TRY(step);
   EDP_TRY(end);
-  EDP_TRY(count_kernels(body, p->kernels_per_round));
+  p->body_graph = body;
   EDP_TRY(stage_rank(d, p->scratch, st));
   EDP_TRY(stage_mesh_index(d, p->scratch, p->point_tree, st));
   EDP_TRY(stage_mesh_emit(d, st));
@@ -376,6 +381,7 @@ int edp_capture(edp_peeler *p) {
   EDP_TRY(e);
   p->graph = g;
   EDP_TRY(count_kernels(g, p->kernels_outside));
+  EDP_TRY(count_kernels(p->body_graph, p->kernels_per_round));
   EDP_TRY(cudaGraphInstantiate(&p->exec, g, 0));
   return EDP_OK;
 }
@@ -482,6 +488,7 @@ int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round) 
 }
 
 int edp_last_cuda_error(void) { return g_last_cuda; }
+const char *edp_last_error_site(void) { return g_last_site; }
 int edp_abi_version(void) { return 1; }
 
 }  // extern "C"

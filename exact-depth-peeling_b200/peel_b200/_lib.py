@@ -43,7 +43,7 @@ EXPORTS = (
     "edp_event_create", "edp_device_create", "edp_event_default_capacities",
     "edp_device_default_capacities", "edp_warmup", "edp_enqueue", "edp_capture", "edp_run",
     "edp_read_status", "edp_get_outputs", "edp_destroy", "edp_status_string",
-    "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
+    "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels", "edp_last_error_site",
 )
 
 _lib = None
@@ -84,6 +84,7 @@ def load():
     lib.edp_status_string.argtypes = [ctypes.c_int]
     lib.edp_status_string.restype = ctypes.c_char_p
     lib.edp_last_cuda_error.restype = ctypes.c_int
+    lib.edp_last_error_site.restype = ctypes.c_char_p
     lib.edp_abi_version.restype = ctypes.c_int
     _lib = lib
     return lib
@@ -102,5 +103,6 @@ def check(code, what):
     if code == 1:
         raise ValueError(f"{what}: {text}")
     if code == 3:
-        raise NativeError(f"{what}: {text} (cudaError {lib.edp_last_cuda_error()})")
+        site = lib.edp_last_error_site().decode()
+        raise NativeError(f"{what}: {text} (cudaError {lib.edp_last_cuda_error()} at {site})")
     raise RuntimeError(f"{what}: {text}")

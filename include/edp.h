@@ -142,6 +142,8 @@ int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
 /* Human-readable edp_status; the last CUDA error code of this thread. */
 const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
+/* Source location ("file:line") of the CUDA call behind the last EDP_ERR_CUDA. */
+const char *edp_last_error_site(void);
 int edp_abi_version(void);
 
 #ifdef __cplusplus
