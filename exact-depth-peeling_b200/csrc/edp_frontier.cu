@@ -170,7 +170,9 @@ cudaError_t stage_step(const Dev &d, cudaStream_t st) {
   int64_t g = ceil_div(d.cap.frontier, kBlock);
   if (g > 148 * 32) g = 148 * 32;
   k_subdivide<<<unsigned(g), kBlock, 0, st>>>(d);
+  note_launch();
   k_advance<<<1, 1, 0, st>>>(d);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -185,3 +185,10 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
 cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st);
 
 }  // namespace edp
+
+namespace edp {
+// Host-side count of kernel launches issued by this thread (every launch site
+// calls note_launch), used to report how many kernels a captured graph runs.
+void note_launch();
+int64_t launch_count();
+}  // namespace edp

@@ -161,9 +161,12 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
                              cudaStream_t st) {
   const int64_t R = d.cap.regions;
   k_mesh_counts<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
   k_mesh_check<<<1, 1, 0, st>>>(d);
+  note_launch();
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kLiveVertices, 0, true, s, st));
   return cudaGetLastError();
 }
@@ -171,6 +174,7 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
 cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st) {
   int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
   k_mesh_edges<<<blocks(d.cap.vertices), kBlock, 0, st>>>(d, cap);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -387,6 +387,7 @@ unsigned blocks(int64_t n) {
 cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
                           TreeBuffers &seg_tree, cudaStream_t st) {
   k_reset<<<1, 32, 0, st>>>(d);
+  note_launch();
   EDP_CHECK(cudaMemsetAsync(d.weld_table, 0xff, sizeof(int) * (int64_t(d.weld_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.weld_min, 0x7f, sizeof(int) * (int64_t(d.weld_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.ekey_table, 0xff, sizeof(unsigned long long) * (int64_t(d.ekey_mask) + 1), st));
@@ -397,21 +398,31 @@ cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree
   EDP_CHECK(cudaMemsetAsync(d.seg_za, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.seg_zb, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
   k_validate<<<blocks(std::max(d.nv, d.n)), kBlock, 0, st>>>(d);
+  note_launch();
   if (d.nv > 0) {
     k_weld_insert<<<blocks(d.nv), kBlock, 0, st>>>(d);
+    note_launch();
     k_weld_resolve<<<blocks(d.nv), kBlock, 0, st>>>(d);
+    note_launch();
   }
   if (d.n > 0) {
     k_project<<<blocks(d.n), kBlock, 0, st>>>(d);
+    note_launch();
     k_edge_insert<<<blocks(3 * int64_t(d.n)), kBlock, 0, st>>>(d);
+    note_launch();
     k_edge_mark<<<blocks(3 * int64_t(d.n)), kBlock, 0, st>>>(d);
+    note_launch();
     k_segments<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+    note_launch();
     k_segment_bounds<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+    note_launch();
   }
   EDP_CHECK(tree_build(source_tree, d.src_lo, d.src_hi, nullptr, d.n, false, s, st));
   EDP_CHECK(tree_build(seg_tree, d.seg_lo, d.seg_hi, nullptr, kSourceVertices * d.n, false, s, st));
   k_seed<<<blocks(d.n), kBlock, 0, st>>>(d);
+  note_launch();
   k_loop_condition<<<1, 1, 0, st>>>(d);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -221,14 +221,17 @@ cudaError_t sort_pairs(K *keys, K *keys_tmp, int *vals, int *vals_tmp, const int
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     k_radix_hist<K><<<unsigned(tiles), kSortBlock, 0, st>>>(ka, count, s.tiles, shift, s.hist);
+    note_launch();
     k_radix_scan<<<256, 256, 0, st>>>(s.hist, count, s.tiles, s.totals);
-    k_radix_scatter<K><<<unsigned(tiles), kSortBlock, 0, st>>>(ka, va, kb, vb, count, s.tiles,
-                                                               shift, s.hist, s.totals);
+    note_launch();
+    k_radix_scatter<K><<<unsigned(tiles), kSortBlock, 0, st>>>(ka, va, kb, vb, count, s.tiles, shift, s.hist, s.totals);
+    note_launch();
     K *tk = ka; ka = kb; kb = tk;
     int *tv = va; va = vb; vb = tv;
   }
   if (ka != keys)
     k_copy_pairs<K><<<592, 256, 0, st>>>(ka, va, keys, vals, count);
+    note_launch();
   return cudaGetLastError();
 }
 
@@ -312,8 +315,11 @@ cudaError_t scan_exclusive(const int *in, int *out, const int *count, int64_t ca
   const int64_t tiles = ceil_div(capacity > 0 ? capacity : 1, kScanTile);
   if (tiles > s.scan_tiles) return cudaErrorInvalidValue;
   k_scan_reduce<<<unsigned(tiles), 256, 0, st>>>(in, count, s.partials);
+  note_launch();
   k_scan_partials<<<1, 1024, 0, st>>>(s.partials, count);
+  note_launch();
   k_scan_apply<<<unsigned(tiles), 256, 0, st>>>(in, out, count, s.partials, total);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -356,13 +362,25 @@ void tree_free(TreeBuffers &t) {
 cudaError_t tree_build(TreeBuffers &t, const float4 *lo, const float4 *hi, const int *count_ptr,
                        int static_count, bool layered, SortScratch &s, cudaStream_t st) {
   k_tree_size<<<1, 1, 0, st>>>(count_ptr, static_count, t.count, t.size);
+  note_launch();
   const unsigned g = grid_for(t.leaves_cap, 256) < 4 * 148 ? grid_for(t.leaves_cap, 256) : 4 * 148;
   k_tree_keys<<<g, 256, 0, st>>>(lo, hi, t.count, t.size, t.keys, t.ids, layered ? 1 : 0);
+  note_launch();
   int bits = layered ? 64 : 30;
   EDP_CHECK(sort_pairs_u64(t.keys, t.keys_tmp, t.ids, t.ids_tmp, t.count, t.leaves_cap, bits, s, st));
   k_tree_leaves<<<g, 256, 0, st>>>(t.lo, t.hi, t.ids, lo, hi, t.count, t.size, t.flags);
+  note_launch();
   k_tree_refit<<<g, 256, 0, st>>>(t.lo, t.hi, t.size, t.flags);
+  note_launch();
   return cudaGetLastError();
 }
 
+}  // namespace edp
+
+namespace edp {
+namespace {
+thread_local int64_t g_launches = 0;
+}
+void note_launch() { ++g_launches; }
+int64_t launch_count() { return g_launches; }
 }  // namespace edp

@@ -543,41 +543,61 @@ int bits_for(int64_t n) {
 cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   const int64_t R = d.cap.regions, E = d.cap.vertices;
   k_rank_begin<<<1, 1, 0, st>>>(d);
+  note_launch();
   k_polygon_init<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   const bool connected = d.propagate_ranks || d.merge_regions;
   if (connected) {
     EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kPatchEdges, s, st));
     k_check_edges<<<1, 1, 0, st>>>(d);
+    note_launch();
     k_patch_edges<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
     EDP_CHECK(cudaMemsetAsync(d.edge_hash, 0xff, sizeof(int) * (int64_t(d.edge_hash_mask) + 1), st));
     k_match_edges<<<blocks(E), kBlock, 0, st>>>(d);
+    note_launch();
     if (d.propagate_ranks) k_connect<<<blocks(E), kBlock, 0, st>>>(d);
+    note_launch();
   }
   k_roots<<<blocks(R), kBlock, 0, st>>>(d, d.propagate_ranks ? 1 : 0);
+  note_launch();
   k_samples<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   EDP_CHECK(cudaMemsetAsync(d.sample_table, 0xff, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.sample_min, 0x7f, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
   k_cells_reset<<<kCells / 128, 128, 0, st>>>(d);
+  note_launch();
   k_group_insert<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   k_group_resolve<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   if (d.share_regions) {
     k_certify<<<kCells / 128, 128, 0, st>>>(d);
+    note_launch();
     k_certify_heavy<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+    note_launch();
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
   }
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   k_heavy_hits<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+  note_launch();
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
   k_check_hits<<<1, 1, 0, st>>>(d);
+  note_launch();
   const int pass_bits[3] = {bits_for(d.n), 64, bits_for(R)};
   for (int stage = 0; stage < 3; ++stage) {
     k_hit_keys<<<blocks(d.cap.hits), kBlock, 0, st>>>(d, stage);
+    note_launch();
     EDP_CHECK(sort_pairs_u64(reinterpret_cast<uint64_t *>(d.hkeys),
                              reinterpret_cast<uint64_t *>(d.hkeys_tmp), d.hit_ids, d.hit_ids_tmp,
                              d.sc + kLiveHits, d.cap.hits, pass_bits[stage], s, st));
   }
   k_layers_reset<<<1, 1, 0, st>>>(d);
+  note_launch();
   k_assign<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -29,7 +29,6 @@ struct edp_peeler {
   bool warmed = false;
   int device = 0;
   cudaGraphExec_t stage_exec[kStages] = {};
-  cudaGraph_t body_graph = nullptr;  // loop body of the last own capture (owned by graph)
   // Kernel nodes of the last capture: outside the subdivision loop, and in
   // one iteration of its body.
   int64_t kernels_outside = 0, kernels_per_round = 0;
@@ -39,21 +38,6 @@ namespace {
 
 thread_local int g_last_cuda = 0;
 thread_local const char *g_last_site = "";
-
-cudaError_t count_kernels(cudaGraph_t g, int64_t &count) {
-  size_t n = 0;
-  cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
-  if (e != cudaSuccess) return e;
-  std::vector<cudaGraphNode_t> nodes(n);
-  if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
-  count = 0;
-  for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
-    cudaGraphNodeType t;
-    e = cudaGraphNodeGetType(nodes[i], &t);
-    count += t == cudaGraphNodeTypeKernel;
-  }
-  return e;
-}
 
 int cuda_fail(cudaError_t e, const char *site) {
   g_last_cuda = int(e);
@@ -226,6 +210,7 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
   d.use_handle = 1;
   d.cond_handle = handle;
+  const int64_t first_launch = launch_count();
   EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
   EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
@@ -240,15 +225,18 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies));
   EDP_TRY(cudaStreamBeginCaptureToGraph(p->body_stream, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeRelaxed));
+  const int64_t body_first = launch_count();
   cudaError_t step = stage_step(d, p->body_stream);
+  const int64_t per_round = launch_count() - body_first;
   cudaGraph_t captured = nullptr;
   cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
   EDP_TRY(step);
   EDP_TRY(end);
-  p->body_graph = body;
   EDP_TRY(stage_rank(d, p->scratch, st));
   EDP_TRY(stage_mesh_index(d, p->scratch, p->point_tree, st));
   EDP_TRY(stage_mesh_emit(d, st));
+  p->kernels_per_round = per_round;
+  p->kernels_outside = launch_count() - first_launch - per_round;
   return EDP_OK;
 }
 
@@ -380,8 +368,6 @@ int edp_capture(edp_peeler *p) {
   }
   EDP_TRY(e);
   p->graph = g;
-  EDP_TRY(count_kernels(g, p->kernels_outside));
-  EDP_TRY(count_kernels(p->body_graph, p->kernels_per_round));
   EDP_TRY(cudaGraphInstantiate(&p->exec, g, 0));
   return EDP_OK;
 }
