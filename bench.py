@@ -169,14 +169,15 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from peel_b200 import EventPeeler, _lib, scenes
+    from peel_b200 import _lib, scenes
+    from peel_b200.sizing import fit_event_capacities
 
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
     host = scenes.CONFIGS[args.config]()
     vertices, faces, camera, settings = host
     arrays = scenes.to_device(host, device)
-    p = EventPeeler(*arrays)
+    p, capacities = fit_event_capacities(arrays)
     lib = _lib.load()
     p.capture()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
@@ -286,6 +287,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": None, "clocks": clocks.summary(),
         "stages_ms": stage_ms,
         "output": {k: check[k] for k in ("polygons", "triangles", "layers", "boundary_vertices")},
+        "capacities": vars(capacities),
     }
     outside = np.zeros(2, dtype=np.int64)
     _lib.check(lib.edp_graph_kernels(p._ws.handle, outside.ctypes.data, outside.ctypes.data + 8),
