@@ -16,10 +16,21 @@ _POOL_OF_BIT = {4: "frontier", 8: "regions", 16: "vertices", 32: "triangles", 64
                 1024: "hits", 2048: "rounds"}
 
 
-def fit_event_capacities(arrays, capacities=None, attempts=8, **options):
-    """Return (peeler, capacities) whose extraction of ``arrays`` does not overflow.
+def _usage(p):
+    """Observed use of each pool by the last extraction (status/metrics slots)."""
+    status = p.status.cpu().numpy()
+    metrics = p.metrics.cpu().numpy()
+    return {"frontier": int(status[12]), "regions": int(status[2]), "vertices": int(status[6]),
+            "triangles": int(status[3]), "hits": int(metrics[5]), "rounds": int(metrics[6])}
 
-    Bits that no capacity can fix (invalid input, polygon vertices, edge noding)
+
+def fit_event_capacities(arrays, capacities=None, attempts=8, headroom=2.0, **options):
+    """Return (peeler, capacities) whose extraction of ``arrays`` does not
+    overflow, with ``headroom`` x the observed use of every pool.
+
+    Atomic appends make the polygon order, and with it the query grouping and
+    the hit count, vary slightly between replays, hence the headroom.  Bits
+    that no capacity can fix (invalid input, polygon vertices, edge noding)
     raise immediately."""
     cap = capacities or EventCapacities.for_mesh(arrays[1].shape[0])
     for _ in range(attempts):
@@ -27,7 +38,14 @@ def fit_event_capacities(arrays, capacities=None, attempts=8, **options):
         p.run()
         error = int(p.status[9].item())  # synchronising read of the sticky error bits
         if error == 0:
-            return p, cap
+            used = _usage(p)
+            tight = {f: max(getattr(cap, f) * 2, int(headroom * used[f]))
+                     for f in used if used[f] * headroom > getattr(cap, f)}
+            if not tight:
+                return p, cap
+            del p
+            cap = replace(cap, **tight)
+            continue
         grow = {f: getattr(cap, f) * 2 for b, f in _POOL_OF_BIT.items() if error & b}
         if not grow or error & ~sum(_POOL_OF_BIT):
             p.read_status()  # raises with the reference's message
