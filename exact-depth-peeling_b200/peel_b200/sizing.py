@@ -17,7 +17,8 @@ _POOL_OF_BIT = {4: "frontier", 8: "regions", 16: "vertices", 32: "triangles", 64
 
 
 def _usage(p):
-    """Observed use of each pool by the last extraction (status/metrics slots)."""
+    """Observed use of each pool by the last extraction (status/metrics slots).
+    The caller has synchronised the workspace stream."""
     status = p.status.cpu().numpy()
     metrics = p.metrics.cpu().numpy()
     return {"frontier": int(status[12]), "regions": int(status[2]), "vertices": int(status[6]),
@@ -36,7 +37,8 @@ def fit_event_capacities(arrays, capacities=None, attempts=8, headroom=2.0, **op
     for _ in range(attempts):
         p = EventPeeler(*arrays, capacities=cap, **options)
         p.run()
-        error = int(p.status[9].item())  # synchronising read of the sticky error bits
+        p.stream.synchronize()  # the views live on the workspace stream
+        error = int(p.status[9].item())
         if error == 0:
             used = _usage(p)
             tight = {f: max(getattr(cap, f) * 2, int(headroom * used[f]))
