@@ -8,7 +8,10 @@ namespace edp {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kHeavyWorkers = 8192;  // persistent continuation workers (events.py:510,564)
+// Persistent continuation grid: 8 blocks of 256 threads on each of the 148 SMs
+// (the reference launches 8192 workers, events.py:510,564, sized for a smaller part).
+constexpr int kHeavyBlock = 256;
+constexpr int kHeavyBlocks = 148 * 8;
 constexpr int kCells = 1024;         // 32 x 32 image buckets (beams.py:18-22)
 
 __device__ inline int64_t tid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
@@ -574,14 +577,14 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   if (d.share_regions) {
     k_certify<<<kCells / 128, 128, 0, st>>>(d);
     note_launch();
-    k_certify_heavy<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+    k_certify_heavy<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
     note_launch();
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
     note_launch();
   }
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
-  k_heavy_hits<<<kHeavyWorkers / 128, 128, 0, st>>>(d);
+  k_heavy_hits<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
   k_check_hits<<<1, 1, 0, st>>>(d);
