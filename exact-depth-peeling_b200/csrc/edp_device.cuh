@@ -6,6 +6,9 @@
 // is compiled with -fmad=false, so every predicate is plain IEEE binary64 and a
 // CPU restatement of the same expression gives the same bits.
 #pragma once
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -251,5 +254,38 @@ __device__ inline double atomic_max_double(double *addr, double v) {
 }
 
 __device__ inline void set_error(int *status, int bit) { atomicOr(&status[kError], bit); }
+
+// Reserve `count` consecutive slots of an append counter for this thread,
+// with a single atomic per group of converged threads (the group's scan gives
+// each thread its offset).  Avoids serialising millions of appends on one
+// address.
+__device__ inline int reserve(int *counter, int count) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  int offset = cg::exclusive_scan(g, count);
+  int total = g.shfl(offset + count, g.size() - 1);
+  int base = 0;
+  if (g.thread_rank() == 0 && total) base = atomicAdd(counter, total);
+  return g.shfl(base, 0) + offset;
+}
+__device__ inline long long reserve(long long *counter, int count) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  int offset = cg::exclusive_scan(g, count);
+  int total = g.shfl(offset + count, g.size() - 1);
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0 && total)
+    base = atomicAdd(reinterpret_cast<unsigned long long *>(counter),
+                     static_cast<unsigned long long>(total));
+  return static_cast<long long>(g.shfl(base, 0)) + offset;
+}
+// Add to a counter with one atomic per group of converged threads.
+__device__ inline void count_add(long long *counter, long long v) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  long long total = cg::reduce(g, v, cg::plus<long long>());
+  if (g.thread_rank() == 0 && total)
+    atomicAdd(reinterpret_cast<unsigned long long *>(counter), static_cast<unsigned long long>(total));
+}
 
 }  // namespace edp

@@ -27,27 +27,15 @@ __device__ inline bool front_segment(const V2 *p, int n, V2 a, V2 b, double za, 
   return high > low;
 }
 
-__device__ inline void save_output(const Dev &d, const V2 *p, int n, int source) {
-  int slot = atomicAdd(&d.status[kPolygons], 1);
-  if (slot < d.cap.regions) {
-    V2 *dst = d.out_v + int64_t(kMaxVertices) * slot;
-    for (int j = 0; j < n; ++j) dst[j] = p[j];
-    d.out_n[slot] = n;
-    d.out_src[slot] = source;
-    d.out_layer[slot] = 0;
-    atomicMax(&d.status[kLayers], 1);
-  } else {
-    set_error(d.status, kErrOutput);
-  }
-}
-
 // One frontier round.  Each patch visits at most kCandidatesPerPass contour
 // segments of the segment hierarchy, continuing from its cursor.  The first
 // segment that crosses the patch interior and is nearer somewhere splits the
 // patch along its supporting line into two next-round patches that inherit the
 // cursor; a patch whose traversal completes is final and goes to the output
-// pool (frontier.py:106-223).
+// pool; otherwise it carries over (frontier.py:106-223).  Slots are reserved
+// once per converged group of threads and counters are flushed once per thread.
 __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
+  enum Action { kSkip = 0, kSplit = 1, kCarry = 2, kDone = 3 };
   const int par = *d.parity;
   const V2 *fv = d.fv[par];
   const int *fn = d.fn[par], *fsrc = d.fsrc[par], *fcur = d.fcur[par];
@@ -55,12 +43,13 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
   int *nn = d.fn[par ^ 1], *nsrc = d.fsrc[par ^ 1], *ncur = d.fcur[par ^ 1];
   const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
   const int leaves = *d.seg_tree.size;
+  long long visits = 0, tests = 0, splits = 0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < live;
        i += int64_t(gridDim.x) * blockDim.x) {
     if (d.status[kError] != 0) return;
     const int n = fn[i];
     if (n == 0) continue;
-    atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kTargetVisits]), 1ull);
+    ++visits;
     const int source = fsrc[i];
     int node = fcur[i];
     const V2 *p = fv + int64_t(kMaxVertices) * i;
@@ -68,16 +57,18 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
     float4 lo, hi;
     polygon_bounds(p, n, sc, lo, hi);
     lo.z = -1.0e30f;
-    bool done = false, moved = false;
+    int action = kCarry;
+    V2 a = v2(0.0, 0.0), b = a;
     for (int task = 0; task < kCandidatesPerPass; ++task) {
       int c;
       node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
       if (c < 0) {
-        done = true;
+        action = kDone;
         break;
       }
-      atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kContourTests]), 1ull);
-      const V2 a = d.seg_a[c], b = d.seg_b[c];
+      ++tests;
+      a = d.seg_a[c];
+      b = d.seg_b[c];
       bool positive = false, negative = false;
       for (int j = 0; j < n; ++j) {
         double side = cross(a, b, p[j]);
@@ -87,67 +78,82 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
       if (!(positive && negative)) continue;
       const V2 near = d.seg_near[c];
       double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
-      if (!front_segment(p, n, a, b, za, zb)) continue;
-      int slot = atomicAdd(&d.status[kNextResidual], 2);
-      if (int64_t(slot) + 1 >= d.cap.frontier) {
+      if (front_segment(p, n, a, b, za, zb)) {
+        action = kSplit;
+        break;
+      }
+    }
+    const int slot = reserve(&d.status[kNextResidual],
+                             action == kSplit ? 2 : action == kCarry ? 1 : 0);
+    const int out = reserve(&d.status[kPolygons], action == kDone ? 1 : 0);
+    if (action == kDone) {
+      if (out >= d.cap.regions) {
+        set_error(d.status, kErrOutput);
+        continue;
+      }
+      V2 *dst = d.out_v + int64_t(kMaxVertices) * out;
+      for (int j = 0; j < n; ++j) dst[j] = p[j];
+      d.out_n[out] = n;
+      d.out_src[out] = source;
+      d.out_layer[out] = 0;
+      continue;
+    }
+    if (action == kCarry) {
+      if (slot >= d.cap.frontier) {
         set_error(d.status, kErrResidual);
-        return;
+        continue;
       }
-      V2 *left_v = nv + int64_t(kMaxVertices) * slot;
-      V2 *right_v = left_v + kMaxVertices;
-      int left = 0, right = 0;
-      V2 dir = b - a;
-      Plane s{-dir.y, dir.x, 0.0, 0.0};
-      for (int j = 0; j < n; ++j) {
-        V2 u = p[j], v = p[(j + 1) % n];
-        double du = value(s, u - a), dv = value(s, v - a);
-        if (du >= 0.0) left = append(left_v, left, u);
-        if (du <= 0.0) right = append(right_v, right, u);
-        if ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0)) {
-          V2 x = u + (du / (du - dv)) * (v - u);
-          left = append(left_v, left, x);
-          right = append(right_v, right, x);
-        }
-      }
-      left = clean(left_v, left);
-      right = clean(right_v, right);
-      if (left > kMaxVertices || right > kMaxVertices) {
-        set_error(d.status, kErrPolygon);
-        return;
-      }
-      if (left > 0 && right > 0) {
-        atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kSplits]), 1ull);
-      } else {
-        // A collapsed child cancels this cut; the parent continues next round.
-        left = n;
-        right = 0;
-        for (int j = 0; j < n; ++j) left_v[j] = p[j];
-      }
-      nn[slot] = left;
-      nn[slot + 1] = right;
+      V2 *dst = nv + int64_t(kMaxVertices) * slot;
+      for (int j = 0; j < n; ++j) dst[j] = p[j];
+      nn[slot] = n;
       nsrc[slot] = source;
-      nsrc[slot + 1] = source;
       ncur[slot] = node;
-      ncur[slot + 1] = node;
-      moved = true;
-      break;
+      continue;
     }
-    if (moved) continue;
-    if (done) {
-      save_output(d, p, n, source);
-    } else {
-      int slot = atomicAdd(&d.status[kNextResidual], 1);
-      if (slot < d.cap.frontier) {
-        V2 *dst = nv + int64_t(kMaxVertices) * slot;
-        for (int j = 0; j < n; ++j) dst[j] = p[j];
-        nn[slot] = n;
-        nsrc[slot] = source;
-        ncur[slot] = node;
-      } else {
-        set_error(d.status, kErrResidual);
+    if (int64_t(slot) + 1 >= d.cap.frontier) {
+      set_error(d.status, kErrResidual);
+      continue;
+    }
+    V2 *left_v = nv + int64_t(kMaxVertices) * slot;
+    V2 *right_v = left_v + kMaxVertices;
+    int left = 0, right = 0;
+    V2 dir = b - a;
+    Plane s{-dir.y, dir.x, 0.0, 0.0};
+    for (int j = 0; j < n; ++j) {
+      V2 u = p[j], v = p[(j + 1) % n];
+      double du = value(s, u - a), dv = value(s, v - a);
+      if (du >= 0.0) left = append(left_v, left, u);
+      if (du <= 0.0) right = append(right_v, right, u);
+      if ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0)) {
+        V2 x = u + (du / (du - dv)) * (v - u);
+        left = append(left_v, left, x);
+        right = append(right_v, right, x);
       }
     }
+    left = clean(left_v, left);
+    right = clean(right_v, right);
+    if (left > kMaxVertices || right > kMaxVertices) {
+      set_error(d.status, kErrPolygon);
+      continue;
+    }
+    if (left > 0 && right > 0) {
+      ++splits;
+    } else {
+      // A collapsed child cancels this cut; the parent continues next round.
+      left = n;
+      right = 0;
+      for (int j = 0; j < n; ++j) left_v[j] = p[j];
+    }
+    nn[slot] = left;
+    nn[slot + 1] = right;
+    nsrc[slot] = source;
+    nsrc[slot + 1] = source;
+    ncur[slot] = node;
+    ncur[slot + 1] = node;
   }
+  count_add(&d.metrics[kTargetVisits], visits);
+  count_add(&d.metrics[kContourTests], tests);
+  count_add(&d.metrics[kSplits], splits);
 }
 
 // Swap frontiers and decide whether another round runs (event_kernels.py:12-25).

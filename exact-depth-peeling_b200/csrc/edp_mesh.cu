@@ -120,31 +120,55 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
       }
       params[m + 1] = v;
     }
+    // Count this edge's fan triangles, reserve their slots at once, then emit.
+    int emitted = 0;
+    {
+      double previous = 0.0;
+      V2 cursor = a;
+      for (int step = 0; step <= count; ++step) {
+        double following = step < count ? params[step] : 1.0;
+        if (following <= previous + kEps) continue;
+        V2 next = a + following * dir;
+        if (fabs(cross(center, cursor, next)) > kEps * kEps) ++emitted;
+        cursor = next;
+        previous = following;
+      }
+    }
+    int slot = reserve(&d.status[kTriangles], emitted);
+    if (int64_t(slot) + emitted > d.cap.triangles) {
+      set_error(d.status, kErrTriangles);
+      continue;
+    }
     const Plane sc = d.scores[source];
+    double w_center[3];
+    lift(d, center, sc, w_center);
     double previous = 0.0;
     V2 cursor = a;
+    double w_cursor[3];
+    lift(d, cursor, sc, w_cursor);
     for (int step = 0; step <= count; ++step) {
       double following = step < count ? params[step] : 1.0;
       if (following <= previous + kEps) continue;
       V2 next = a + following * dir;
+      double w_next[3];
+      lift(d, next, sc, w_next);
       if (fabs(cross(center, cursor, next)) > kEps * kEps) {
-        int slot = atomicAdd(&d.status[kTriangles], 1);
-        if (slot < d.cap.triangles) {
-          V2 *uv = d.tri_uv + 3 * int64_t(slot);
-          double *w = d.tri_world + 9 * int64_t(slot);
-          uv[0] = center;
-          uv[1] = cursor;
-          uv[2] = next;
-          lift(d, center, sc, w);
-          lift(d, cursor, sc, w + 3);
-          lift(d, next, sc, w + 6);
-          d.tri_src[slot] = source;
-          d.tri_layer[slot] = layer;
-        } else {
-          set_error(d.status, kErrTriangles);
+        V2 *uv = d.tri_uv + 3 * int64_t(slot);
+        double *w = d.tri_world + 9 * int64_t(slot);
+        uv[0] = center;
+        uv[1] = cursor;
+        uv[2] = next;
+        for (int k = 0; k < 3; ++k) {
+          w[k] = w_center[k];
+          w[3 + k] = w_cursor[k];
+          w[6 + k] = w_next[k];
         }
+        d.tri_src[slot] = source;
+        d.tri_layer[slot] = layer;
+        ++slot;
       }
       cursor = next;
+      for (int k = 0; k < 3; ++k) w_cursor[k] = w_next[k];
       previous = following;
     }
   }

@@ -16,10 +16,7 @@ constexpr int kCells = 1024;         // 32 x 32 image buckets (beams.py:18-22)
 
 __device__ inline int64_t tid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
 __device__ inline int64_t stride() { return int64_t(gridDim.x) * blockDim.x; }
-__device__ inline void add_metric(const Dev &d, int m, long long v) {
-  atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[m]),
-            static_cast<unsigned long long>(v));
-}
+__device__ inline void add_metric(const Dev &d, int m, long long v) { count_add(&d.metrics[m], v); }
 __device__ inline int live_polygons(const Dev &d) { return d.sc[kLivePolygons]; }
 __device__ inline float lower_f(double x) { return __double2float_rd(x); }
 __device__ inline float upper_f(double x) { return __double2float_ru(x); }
@@ -391,50 +388,65 @@ __device__ inline bool contains_flat(const Dev &d, int source, V2 x) {
   return n > 0;
 }
 
-__device__ inline void store_hit(const Dev &d, int source, int group, V2 x) {
-  long long slot = (long long)atomicAdd(
-      reinterpret_cast<unsigned long long *>(&d.metrics[kRayHits]), 1ull);
-  if (slot < d.cap.hits) {
-    d.hit_depth[slot] = value(d.scores[source], x);
-    d.hit_src[slot] = source;
-    d.hit_group[slot] = group;
-  } else {
-    set_error(d.status, kErrHits);
+// Hits found by one thread, flushed to the shared pool with one reservation.
+struct HitBuffer {
+  static constexpr int kSize = kCandidatesPerPass;
+  int source[kSize];
+  double depth[kSize];
+  int count = 0;
+
+  __device__ void flush(const Dev &d, int group) {
+    long long slot = reserve(&d.metrics[kRayHits], count);
+    if (slot + count > d.cap.hits) {
+      set_error(d.status, kErrHits);
+    } else {
+      for (int k = 0; k < count; ++k) {
+        d.hit_depth[slot + k] = depth[k];
+        d.hit_src[slot + k] = source[k];
+        d.hit_group[slot + k] = group;
+      }
+    }
+    count = 0;
   }
-}
+};
 
 // One ray per group leader: up to kCandidatesPerPass sources, the rest of the
 // traversal is queued for the persistent continuation (event_kernels.py:196-245).
 __global__ void k_ray_hits(Dev d) {
   const int live = live_polygons(d);
   const int leaves = *d.source_tree.size;
+  long long groups = 0, tests = 0;
+  HitBuffer hits;
   for (int64_t i = tid(); i < live; i += stride()) {
     if (d.status[kError] != 0) return;
     if (d.groups[i] != int(i)) continue;
     V2 x = d.samples[i];
     float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
-    int node = 1, count = 0, visits = 0;
+    int node = 1;
     for (int step = 0; step < kCandidatesPerPass; ++step) {
       int s;
       node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
       if (s < 0) break;
-      ++visits;
+      ++tests;
       if (contains_flat(d, s, x)) {
-        store_hit(d, s, int(i), x);
-        ++count;
+        hits.source[hits.count] = s;
+        hits.depth[hits.count] = value(d.scores[s], x);
+        ++hits.count;
       }
       if (node == 0) break;
     }
-    atomicAdd(&d.group_counts[i], count);
-    add_metric(d, kRayGroups, 1);
-    add_metric(d, kRayCandidateTests, visits);
-    if (node > 0) {
+    d.group_counts[i] = hits.count;
+    hits.flush(d, int(i));
+    ++groups;
+    const bool heavy = node > 0;
+    if (heavy)
       while (node < leaves) node *= 2;
-      int slot = int(atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kHeavyRayGroups]), 1ull));
-      d.heavy_queries[slot] = make_int2(int(i), node);
-    }
+    int slot = int(reserve(&d.metrics[kHeavyRayGroups], heavy ? 1 : 0));
+    if (heavy) d.heavy_queries[slot] = make_int2(int(i), node);
   }
+  count_add(&d.metrics[kRayGroups], groups);
+  count_add(&d.metrics[kRayCandidateTests], tests);
 }
 
 __global__ void k_heavy_hits(Dev d) {
@@ -443,6 +455,8 @@ __global__ void k_heavy_hits(Dev d) {
   const long long jobs = d.metrics[kHeavyRayGroups];
   int parts, width;
   heavy_partition(leaves, jobs, parts, width);
+  long long tests = 0;
+  HitBuffer hits;
   for (long long task = tid(); task < jobs * parts; task += stride()) {
     int2 job = d.heavy_queries[task / parts];
     int part = int(task % parts);
@@ -453,20 +467,23 @@ __global__ void k_heavy_hits(Dev d) {
     V2 x = d.samples[i];
     float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
-    int count = 0, visits = 0;
+    int found = 0;
     while (node > 0 && node != end) {
       int s;
       node = query_next(d.source_tree, leaves, lo, hi, node, end, s);
       if (s < 0) break;
-      ++visits;
+      ++tests;
       if (contains_flat(d, s, x)) {
-        store_hit(d, s, i, x);
-        ++count;
+        hits.source[hits.count] = s;
+        hits.depth[hits.count] = value(d.scores[s], x);
+        ++found;
+        if (++hits.count == HitBuffer::kSize) hits.flush(d, i);
       }
     }
-    if (count) atomicAdd(&d.group_counts[i], count);
-    add_metric(d, kRayCandidateTests, visits);
+    if (hits.count) hits.flush(d, i);
+    if (found) atomicAdd(&d.group_counts[i], found);
   }
+  count_add(&d.metrics[kRayCandidateTests], tests);
 }
 
 __global__ void k_check_hits(Dev d) {
