@@ -93,6 +93,7 @@ enum Scalar : int {
   kSourceCount = 4,    // n (constant)
   kSegmentCount = 5,   // 8 n (constant)
   kFrontierLive = 6,   // min(status[0], frontier)
+  kUniqueVertices = 7, // distinct (layer, point) boundary vertices
   kScalarCount = 16
 };
 
@@ -161,8 +162,11 @@ struct Dev {
   unsigned long long *hkeys, *hkeys_tmp;
   int *group_counts, *group_offsets;
   // boundary noding and triangles
-  V2 *bverts;
+  V2 *bverts;      // per polygon vertex slot
   int *blayers;
+  V2 *uverts;      // distinct (layer, point) vertices, indexed by the point hierarchy
+  int *point_table;
+  int point_mask;
   float4 *pt_lo, *pt_hi;
   int2 *mtasks;
   V2 *tri_uv;        // [triangles][3]

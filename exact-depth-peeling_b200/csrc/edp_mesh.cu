@@ -19,6 +19,7 @@ __global__ void k_mesh_counts(Dev d) {
 }
 
 __global__ void k_mesh_check(Dev d) {
+  d.sc[kUniqueVertices] = 0;
   int total = d.sc[kLiveVertices];
   d.status[kBoundaryVertices] = total;
   if (int64_t(total) > d.cap.vertices) {
@@ -27,8 +28,10 @@ __global__ void k_mesh_check(Dev d) {
   }
 }
 
-// Boundary vertices with their layer, one noding task per polygon edge, and
-// the vertices' point boxes at z = layer (kernels.py:953-991, event_kernels.py:504-516).
+// Boundary vertices with their layer and one noding task per polygon edge
+// (kernels.py:953-991, event_kernels.py:504-516).  Each distinct (layer,
+// point) enters the point hierarchy once: a vertex shared by several patches
+// would otherwise be a candidate of every query several times over.
 __global__ void k_scatter(Dev d) {
   const int live = d.sc[kLivePolygons];
   for (int64_t i = tid(); i < live; i += stride()) {
@@ -42,10 +45,28 @@ __global__ void k_scatter(Dev d) {
       d.bverts[slot] = x;
       d.blayers[slot] = layer;
       d.mtasks[slot] = make_int2(int(i), j);
-      d.pt_lo[slot] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
-                                  float(layer), 0.f);
-      d.pt_hi[slot] = make_float4(__double2float_ru(x.x + 2.0e-7), __double2float_ru(x.y + 2.0e-7),
-                                  float(layer), 0.f);
+      __threadfence();  // publish the point before its slot can be found in the table
+      uint64_t h = mix64(mix64(key_bits(x.x)) ^ key_bits(x.y)) ^ mix64(uint64_t(layer) + 7ull);
+      uint32_t probe = uint32_t(h) & uint32_t(d.point_mask);
+      bool fresh = false;
+      for (int k = 0; k <= d.point_mask; ++k) {
+        int cur = atomicCAS(&d.point_table[probe], -1, int(slot));
+        if (cur == -1) {
+          fresh = true;
+          break;
+        }
+        V2 y = v2(__ldcg(&d.bverts[cur].x), __ldcg(&d.bverts[cur].y));
+        if (y == x && __ldcg(&d.blayers[cur]) == layer) break;
+        probe = (probe + 1) & uint32_t(d.point_mask);
+      }
+      int u = reserve(&d.sc[kUniqueVertices], fresh ? 1 : 0);
+      if (fresh) {
+        d.uverts[u] = x;
+        d.pt_lo[u] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
+                                 float(layer), 0.f);
+        d.pt_hi[u] = make_float4(__double2float_ru(x.x + 2.0e-7), __double2float_ru(x.y + 2.0e-7),
+                                 float(layer), 0.f);
+      }
     }
   }
 }
@@ -95,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
       int j;
       node = query_next(d.point_tree, leaves, lo, hi, node, 0, j);
       if (j < 0) break;
-      V2 x = d.bverts[j];
+      V2 x = d.uverts[j];
       double tt = dot(x - a, dir) / length2;
       if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= tol) {
         if (count < edge_capacity) {
@@ -189,9 +210,10 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
   k_mesh_check<<<1, 1, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(cudaMemsetAsync(d.point_table, 0xff, sizeof(int) * (int64_t(d.point_mask) + 1), st));
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
-  EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kLiveVertices, 0, true, s, st));
+  EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
   return cudaGetLastError();
 }
 

@@ -157,6 +157,9 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.hkeys_tmp, H));
   EDP_CHECK(alloc(p, &d.bverts, E));
   EDP_CHECK(alloc(p, &d.blayers, E));
+  EDP_CHECK(alloc(p, &d.uverts, E));
+  d.point_mask = table_mask(E);
+  EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
   EDP_CHECK(alloc(p, &d.pt_lo, E));
   EDP_CHECK(alloc(p, &d.pt_hi, E));
   EDP_CHECK(alloc(p, &d.mtasks, E));
