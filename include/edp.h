@@ -139,6 +139,23 @@ int edp_run_stage(edp_peeler *p, int32_t stage);
  * loop iteration (a replay launches outside + per_round * rounds kernels). */
 int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
 
+/* Exact-position welding without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc where they need
+ * welded ids (while recording a CUDA graph, under an allocator that owns all
+ * device memory, or in a loop that must not allocate after start-up).
+ * canonical[i] receives the smallest index j with vertices[j] equal to
+ * vertices[i] (signed zeros equal) - the same ids as edp_get_outputs'
+ * `canonical`.  Both buffers are the caller's device memory; kernels run on
+ * `stream`.  The hash-table scratch is a fixed 5 MiB device array that every
+ * GPU loading this library holds until the process exits, so nv is limited to
+ * EDP_WELD_NOALLOC_MAX_VERTICES (larger nv returns EDP_ERR_ARGUMENT).  The
+ * first call on a device resolves that array's device address; make it before
+ * any stream capture.  All calls on a device share the array and each call
+ * clears the part it uses first: calls that overlap on the GPU (different
+ * streams, or different host threads) race and give undefined ids. */
+#define EDP_WELD_NOALLOC_MAX_VERTICES 262144
+int edp_weld_noalloc(const double *vertices, int64_t nv, int32_t *canonical, void *stream);
+
 /* Human-readable edp_status; the last CUDA error code of this thread. */
 const char *edp_status_string(int code);
 int edp_last_cuda_error(void);

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     for name in declared():
         assert hasattr(lib, name), name
-    assert set(declared()) <= set(_lib.EXPORTS) | {"edp_create_noalloc"}
+    assert set(declared()) <= set(_lib.EXPORTS) | {"edp_weld_noalloc"}
     assert lib.edp_abi_version() >= 1
     assert lib.edp_status_string(1) == b"invalid argument"
 
