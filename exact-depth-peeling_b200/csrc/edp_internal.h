@@ -174,7 +174,43 @@ struct Dev {
   int *tri_src, *tri_layer;
   unsigned long long cond_handle;  // cudaGraphConditionalHandle of the subdivision loop
   int use_handle;
+
+  // DevicePeeler (iterative clipping) only.
+  float4 *contour_lo, *contour_hi;  // per source: box of its contour edges
+  Tree contour_tree;
+  int *ranks;                       // whole-source rank, -1 = needs clipping
+  V2 *res_v[2];                     // residual patches, ping-pong [residual][32]
+  int *res_n[2], *res_src[2];
+  float4 *res_lo, *res_hi;
+  Tree residual_tree;
+  V2 *pool_v[3];                    // per-worker pieces: visible, temporary, hidden
+  int *pool_n[3];                   // [workers][pieces]
+  long long *stats;                 // [layers][3]: targets, candidate tests, restored whole
+  int workers, pieces;
 };
+
+// Polygon edge `edge` of source `source` is a contour: every edge of a
+// camera-clipped source, else the mesh edge's mark; a back-facing source's
+// polygon was reversed (kernels.py:523-536).
+__device__ inline bool contour_edge(const Dev &d, int64_t source, int edge) {
+  if (d.clipped[source] != 0) return true;
+  int j = edge;
+  if (d.facing[source] < 0) j = (4 - edge) % 3;
+  return d.masks[3 * source + j] != 0;
+}
+
+// Reset, validation, welding, projection, mesh contours and the source
+// hierarchy: the part of preparation both peelers share.
+cudaError_t stage_prepare_common(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                                 cudaStream_t st);
+cudaError_t stage_device_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                                 TreeBuffers &contour_tree, cudaStream_t st);
+cudaError_t stage_device_finish(const Dev &d, cudaStream_t st);
+cudaError_t stage_device_layer(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                               TreeBuffers &residual_tree, cudaStream_t st);
+// Bring the source hierarchy's leaves up to date with its item boxes without
+// re-sorting (solver.py:72-89).
+cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st);
 
 // Stage launchers (edp_kernels.cu).  Each enqueues kernels on `st`.
 cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,

@@ -272,14 +272,6 @@ __global__ void k_edge_mark(Dev d) {
   }
 }
 
-// Polygon edge `edge` of source `source` is a contour (kernels.py:523-536).
-__device__ inline bool contour_edge(const Dev &d, int64_t source, int edge) {
-  if (d.clipped[source] != 0) return true;
-  int j = edge;
-  if (d.facing[source] < 0) j = (4 - edge) % 3;
-  return d.masks[3 * source + j] != 0;
-}
-
 // Up to eight canonical contour segments per source with endpoint depths,
 // deduplicated exactly; each group keeps its per-endpoint minimum depth
 // (event_kernels.py:388-480).  Grouping uses a table instead of four sorts.
@@ -384,19 +376,14 @@ unsigned blocks(int64_t n) {
 
 }  // namespace
 
-cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
-                          TreeBuffers &seg_tree, cudaStream_t st) {
+cudaError_t stage_prepare_common(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                                 cudaStream_t st) {
   k_reset<<<1, 32, 0, st>>>(d);
   note_launch();
   EDP_CHECK(cudaMemsetAsync(d.weld_table, 0xff, sizeof(int) * (int64_t(d.weld_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.weld_min, 0x7f, sizeof(int) * (int64_t(d.weld_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.ekey_table, 0xff, sizeof(unsigned long long) * (int64_t(d.ekey_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.ekey_count, 0, sizeof(int) * (int64_t(d.ekey_mask) + 1), st));
-  EDP_CHECK(cudaMemsetAsync(d.seg_table, 0xff, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
-  EDP_CHECK(cudaMemsetAsync(d.seg_min, 0x7f, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
-  // 0x7f bytes are 1.38e306 as binary64: above every finite depth we store.
-  EDP_CHECK(cudaMemsetAsync(d.seg_za, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
-  EDP_CHECK(cudaMemsetAsync(d.seg_zb, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
   k_validate<<<blocks(std::max(d.nv, d.n)), kBlock, 0, st>>>(d);
   note_launch();
   if (d.nv > 0) {
@@ -412,12 +399,25 @@ cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree
     note_launch();
     k_edge_mark<<<blocks(3 * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();
+  }
+  EDP_CHECK(tree_build(source_tree, d.src_lo, d.src_hi, nullptr, d.n, false, s, st));
+  return cudaGetLastError();
+}
+
+cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
+                          TreeBuffers &seg_tree, cudaStream_t st) {
+  EDP_CHECK(stage_prepare_common(d, s, source_tree, st));
+  EDP_CHECK(cudaMemsetAsync(d.seg_table, 0xff, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
+  EDP_CHECK(cudaMemsetAsync(d.seg_min, 0x7f, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
+  // 0x7f bytes are 1.38e306 as binary64: above every finite depth we store.
+  EDP_CHECK(cudaMemsetAsync(d.seg_za, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
+  EDP_CHECK(cudaMemsetAsync(d.seg_zb, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
+  if (d.n > 0) {
     k_segments<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();
     k_segment_bounds<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();
   }
-  EDP_CHECK(tree_build(source_tree, d.src_lo, d.src_hi, nullptr, d.n, false, s, st));
   EDP_CHECK(tree_build(seg_tree, d.seg_lo, d.seg_hi, nullptr, kSourceVertices * d.n, false, s, st));
   k_seed<<<blocks(d.n), kBlock, 0, st>>>(d);
   note_launch();

@@ -384,3 +384,14 @@ thread_local int64_t g_launches = 0;
 void note_launch() { ++g_launches; }
 int64_t launch_count() { return g_launches; }
 }  // namespace edp
+
+namespace edp {
+cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st) {
+  const unsigned g = grid_for(t.leaves_cap, 256) < 4 * 148 ? grid_for(t.leaves_cap, 256) : 4 * 148;
+  k_tree_leaves<<<g, 256, 0, st>>>(t.lo, t.hi, t.ids, lo, hi, t.count, t.size, t.flags);
+  note_launch();
+  k_tree_refit<<<g, 256, 0, st>>>(t.lo, t.hi, t.size, t.flags);
+  note_launch();
+  return cudaGetLastError();
+}
+}  // namespace edp

@@ -22,7 +22,8 @@ struct edp_peeler {
   cudaStream_t stream = nullptr;
   cudaStream_t body_stream = nullptr;
   SortScratch scratch;
-  TreeBuffers source_tree, seg_tree, point_tree;
+  TreeBuffers source_tree, seg_tree, point_tree;  // seg_tree holds contours for DevicePeeler
+  TreeBuffers residual_tree;
   std::vector<void *> allocations;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -74,10 +75,12 @@ bool caps_valid(const Caps &c) {
   return c.edge_vertices <= 128;
 }
 
-cudaError_t allocate_event(edp_peeler *p) {
+// Buffers both peelers use: control, welding, sources, mesh edges, output
+// polygons, boundary noding, triangles, the source and point hierarchies.
+cudaError_t allocate_shared(edp_peeler *p) {
   Dev &d = p->d;
-  const int64_t n = d.n, nv = d.nv, F = d.cap.frontier, R = d.cap.regions, H = d.cap.hits,
-                E = d.cap.vertices, T = d.cap.triangles, S = int64_t(kSourceVertices) * n;
+  const int64_t n = d.n, nv = d.nv, R = d.cap.regions, E = d.cap.vertices, T = d.cap.triangles,
+                S = int64_t(kSourceVertices) * n;
   EDP_CHECK(alloc(p, &d.status, kStatusSlots));
   EDP_CHECK(alloc(p, &d.metrics, kMetrics));
   EDP_CHECK(alloc(p, &d.sc, kScalarCount));
@@ -103,6 +106,45 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.edge_slot, 3 * n));
   EDP_CHECK(alloc(p, &d.masks, 3 * n));
   EDP_CHECK(alloc(p, &d.edge_keys, 3 * n));
+  EDP_CHECK(alloc(p, &d.out_v, R * kMaxVertices));
+  EDP_CHECK(alloc(p, &d.out_n, R));
+  EDP_CHECK(alloc(p, &d.out_src, R));
+  EDP_CHECK(alloc(p, &d.out_layer, R));
+  EDP_CHECK(alloc(p, &d.counts, R));
+  EDP_CHECK(alloc(p, &d.offsets, R));
+  EDP_CHECK(alloc(p, &d.bverts, E));
+  EDP_CHECK(alloc(p, &d.blayers, E));
+  EDP_CHECK(alloc(p, &d.uverts, E));
+  d.point_mask = table_mask(E);
+  EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
+  EDP_CHECK(alloc(p, &d.pt_lo, E));
+  EDP_CHECK(alloc(p, &d.pt_hi, E));
+  EDP_CHECK(alloc(p, &d.mtasks, E));
+  EDP_CHECK(alloc(p, &d.tri_uv, 3 * T));
+  EDP_CHECK(alloc(p, &d.tri_world, 9 * T));
+  EDP_CHECK(alloc(p, &d.tri_src, T));
+  EDP_CHECK(alloc(p, &d.tri_layer, T));
+  EDP_CHECK(tree_alloc(p->source_tree, n));
+  EDP_CHECK(tree_alloc(p->point_tree, E));
+  d.source_tree = p->source_tree.tree();
+  d.point_tree = p->point_tree.tree();
+  return cudaSuccess;
+}
+
+cudaError_t allocate_scratch(edp_peeler *p, int64_t largest_sort, int64_t largest_scan) {
+  p->scratch.tiles = ceil_div(largest_sort, kSortTile);
+  p->scratch.scan_tiles = ceil_div(largest_scan, kScanTile);
+  EDP_CHECK(alloc(p, &p->scratch.hist, 256 * p->scratch.tiles));
+  EDP_CHECK(alloc(p, &p->scratch.totals, 256));
+  EDP_CHECK(alloc(p, &p->scratch.partials, p->scratch.scan_tiles));
+  return cudaSuccess;
+}
+
+cudaError_t allocate_event(edp_peeler *p) {
+  Dev &d = p->d;
+  const int64_t n = d.n, F = d.cap.frontier, R = d.cap.regions, H = d.cap.hits,
+                E = d.cap.vertices, S = int64_t(kSourceVertices) * n;
+  EDP_CHECK(allocate_shared(p));
   d.seg_mask = table_mask(S);
   EDP_CHECK(alloc(p, &d.seg_a, S));
   EDP_CHECK(alloc(p, &d.seg_b, S));
@@ -120,12 +162,6 @@ cudaError_t allocate_event(edp_peeler *p) {
     EDP_CHECK(alloc(p, &d.fsrc[k], F));
     EDP_CHECK(alloc(p, &d.fcur[k], F));
   }
-  EDP_CHECK(alloc(p, &d.out_v, R * kMaxVertices));
-  EDP_CHECK(alloc(p, &d.out_n, R));
-  EDP_CHECK(alloc(p, &d.out_src, R));
-  EDP_CHECK(alloc(p, &d.out_layer, R));
-  EDP_CHECK(alloc(p, &d.counts, R));
-  EDP_CHECK(alloc(p, &d.offsets, R));
   EDP_CHECK(alloc(p, &d.parents, R));
   EDP_CHECK(alloc(p, &d.reps, R));
   EDP_CHECK(alloc(p, &d.samples, R));
@@ -155,52 +191,78 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.hit_ids_tmp, H));
   EDP_CHECK(alloc(p, &d.hkeys, H));
   EDP_CHECK(alloc(p, &d.hkeys_tmp, H));
-  EDP_CHECK(alloc(p, &d.bverts, E));
-  EDP_CHECK(alloc(p, &d.blayers, E));
-  EDP_CHECK(alloc(p, &d.uverts, E));
-  d.point_mask = table_mask(E);
-  EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
-  EDP_CHECK(alloc(p, &d.pt_lo, E));
-  EDP_CHECK(alloc(p, &d.pt_hi, E));
-  EDP_CHECK(alloc(p, &d.mtasks, E));
-  EDP_CHECK(alloc(p, &d.tri_uv, 3 * T));
-  EDP_CHECK(alloc(p, &d.tri_world, 9 * T));
-  EDP_CHECK(alloc(p, &d.tri_src, T));
-  EDP_CHECK(alloc(p, &d.tri_layer, T));
-  EDP_CHECK(tree_alloc(p->source_tree, n));
   EDP_CHECK(tree_alloc(p->seg_tree, S));
-  EDP_CHECK(tree_alloc(p->point_tree, E));
-  d.source_tree = p->source_tree.tree();
   d.seg_tree = p->seg_tree.tree();
-  d.point_tree = p->point_tree.tree();
   int64_t largest = H;
   for (int64_t v : {p->point_tree.leaves_cap, p->seg_tree.leaves_cap, p->source_tree.leaves_cap, R})
     largest = v > largest ? v : largest;
-  p->scratch.tiles = ceil_div(largest, kSortTile);
-  p->scratch.scan_tiles = ceil_div(R > E ? R : E, kScanTile);
-  EDP_CHECK(alloc(p, &p->scratch.hist, 256 * p->scratch.tiles));
-  EDP_CHECK(alloc(p, &p->scratch.totals, 256));
-  EDP_CHECK(alloc(p, &p->scratch.partials, p->scratch.scan_tiles));
-  return cudaSuccess;
+  return allocate_scratch(p, largest, R > E ? R : E);
 }
 
-// The whole extraction, recorded on `st`.  With `graph` the subdivision loop
-// becomes a conditional WHILE node of the graph being captured on `st`;
-// otherwise the host drives the loop (used by warm-up only).
-int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
+cudaError_t allocate_device(edp_peeler *p) {
+  Dev &d = p->d;
+  const int64_t n = d.n, F = d.cap.frontier, R = d.cap.regions, E = d.cap.vertices,
+                pool = int64_t(d.workers) * d.pieces;
+  EDP_CHECK(allocate_shared(p));
+  EDP_CHECK(alloc(p, &d.contour_lo, n));
+  EDP_CHECK(alloc(p, &d.contour_hi, n));
+  EDP_CHECK(alloc(p, &d.ranks, n));
+  for (int k = 0; k < 2; ++k) {
+    EDP_CHECK(alloc(p, &d.res_v[k], F * kMaxVertices));
+    EDP_CHECK(alloc(p, &d.res_n[k], F));
+    EDP_CHECK(alloc(p, &d.res_src[k], F));
+  }
+  EDP_CHECK(alloc(p, &d.res_lo, F));
+  EDP_CHECK(alloc(p, &d.res_hi, F));
+  for (int k = 0; k < 3; ++k) {
+    EDP_CHECK(alloc(p, &d.pool_v[k], pool * kMaxVertices));
+    EDP_CHECK(alloc(p, &d.pool_n[k], pool));
+  }
+  EDP_CHECK(alloc(p, &d.stats, 3 * d.cap.layers));
+  EDP_CHECK(tree_alloc(p->seg_tree, n));  // the contour hierarchy
+  EDP_CHECK(tree_alloc(p->residual_tree, F));
+  d.contour_tree = p->seg_tree.tree();
+  d.residual_tree = p->residual_tree.tree();
+  int64_t largest = R;
+  for (int64_t v : {p->point_tree.leaves_cap, p->seg_tree.leaves_cap, p->source_tree.leaves_cap,
+                    p->residual_tree.leaves_cap})
+    largest = v > largest ? v : largest;
+  return allocate_scratch(p, largest, R > E ? R : E);
+}
+
+// Stage sequence of each peeler.  The loop body runs while the device sets
+// the condition: subdivision rounds (EventPeeler) or layer passes
+// (DevicePeeler).
+cudaError_t run_prepare(edp_peeler *p, const Dev &d, cudaStream_t st) {
+  return p->method == 0 ? stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st)
+                        : stage_device_prepare(d, p->scratch, p->source_tree, p->seg_tree, st);
+}
+cudaError_t run_body(edp_peeler *p, const Dev &d, cudaStream_t st) {
+  return p->method == 0 ? stage_step(d, st)
+                        : stage_device_layer(d, p->scratch, p->source_tree, p->residual_tree, st);
+}
+cudaError_t run_finish(edp_peeler *p, const Dev &d, cudaStream_t st) {
+  EDP_CHECK(p->method == 0 ? stage_rank(d, p->scratch, st) : stage_device_finish(d, st));
+  EDP_CHECK(stage_mesh_index(d, p->scratch, p->point_tree, st));
+  return stage_mesh_emit(d, st);
+}
+
+// The whole extraction, recorded on `st`.  With `graph` the loop becomes a
+// conditional WHILE node of the graph being captured on `st`; otherwise the
+// host drives the loop (used by warm-up only).
+int enqueue(edp_peeler *p, cudaStream_t st, bool graph) {
   Dev d = p->d;
   if (!graph) {
     d.use_handle = 0;
-    EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
+    EDP_TRY(run_prepare(p, d, st));
     while (true) {
       int cond = 0;
       EDP_TRY(cudaMemcpyAsync(&cond, d.condition, sizeof(int), cudaMemcpyDeviceToHost, st));
       EDP_TRY(cudaStreamSynchronize(st));
       if (!cond) break;
-      EDP_TRY(stage_step(d, st));
+      EDP_TRY(run_body(p, d, st));
     }
-    EDP_TRY(stage_rank(d, p->scratch, st));
-    EDP_TRY(stage_mesh(d, p->scratch, p->point_tree, st));
+    EDP_TRY(run_finish(p, d, st));
     return EDP_OK;
   }
   cudaStreamCaptureStatus cs;
@@ -214,7 +276,7 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   d.use_handle = 1;
   d.cond_handle = handle;
   const int64_t first_launch = launch_count();
-  EDP_TRY(stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, st));
+  EDP_TRY(run_prepare(p, d, st));
   EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
   cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
@@ -229,15 +291,13 @@ int enqueue_events(edp_peeler *p, cudaStream_t st, bool graph) {
   EDP_TRY(cudaStreamBeginCaptureToGraph(p->body_stream, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeRelaxed));
   const int64_t body_first = launch_count();
-  cudaError_t step = stage_step(d, p->body_stream);
+  cudaError_t step = run_body(p, d, p->body_stream);
   const int64_t per_round = launch_count() - body_first;
   cudaGraph_t captured = nullptr;
   cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
   EDP_TRY(step);
   EDP_TRY(end);
-  EDP_TRY(stage_rank(d, p->scratch, st));
-  EDP_TRY(stage_mesh_index(d, p->scratch, p->point_tree, st));
-  EDP_TRY(stage_mesh_emit(d, st));
+  EDP_TRY(run_finish(p, d, st));
   p->kernels_per_round = per_round;
   p->kernels_outside = launch_count() - first_launch - per_round;
   return EDP_OK;
@@ -331,14 +391,57 @@ int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, i
 int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
                       const double *camera, const double *settings,
                       const edp_device_capacities *cap, int32_t layers, void *stream,
-                      edp_peeler **out);
+                      edp_peeler **out) {
+  if (!out) return EDP_ERR_ARGUMENT;
+  *out = nullptr;
+  int rc = check_inputs(vertices, nv, faces, nf, camera, settings, stream);
+  if (rc) return rc;
+  edp_device_capacities c;
+  if (cap)
+    c = *cap;
+  else
+    edp_device_default_capacities(nf, &c);
+  // Residual patches use the frontier slot; no ray hits or round cap.
+  Caps caps{c.residual, c.polygons, 1, c.vertices, c.triangles, 1, c.layers, c.edge_vertices};
+  if (!caps_valid(caps) || c.workers < 1 || c.pieces_per_worker < 1 ||
+      c.workers > (int64_t(1) << 24) || c.pieces_per_worker > (int64_t(1) << 20) ||
+      c.workers * c.pieces_per_worker > (int64_t(1) << 30))
+    return EDP_ERR_ARGUMENT;
+  if (layers < 0 || layers > c.layers) return EDP_ERR_ARGUMENT;
+  edp_peeler *p = new edp_peeler();
+  p->method = 1;
+  p->stream = static_cast<cudaStream_t>(stream);
+  Dev &d = p->d;
+  d.vertices = vertices;
+  d.faces = faces;
+  d.camera = camera;
+  d.settings = settings;
+  d.nv = int(nv);
+  d.n = int(nf);
+  d.cap = caps;
+  d.limit = layers ? layers : int(c.layers);
+  d.all_layers = layers == 0;
+  d.workers = int(c.workers);
+  d.pieces = int(c.pieces_per_worker);
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = allocate_device(p);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    edp_destroy(p);
+    g_last_cuda = int(e);
+    return e == cudaErrorMemoryAllocation ? EDP_ERR_MEMORY : EDP_ERR_CUDA;
+  }
+  *out = p;
+  return EDP_OK;
+}
 
 int edp_warmup(edp_peeler *p) {
   if (!p) return EDP_ERR_ARGUMENT;
   cudaStreamCaptureStatus cs;
   EDP_TRY(cudaStreamIsCapturing(p->stream, &cs));
   if (cs != cudaStreamCaptureStatusNone) return EDP_ERR_STATE;
-  int rc = enqueue_events(p, p->stream, false);
+  int rc = enqueue(p, p->stream, false);
   if (rc) return rc;
   EDP_TRY(cudaStreamSynchronize(p->stream));
   p->warmed = true;
@@ -351,7 +454,7 @@ int edp_enqueue(edp_peeler *p, void *stream) {
   cudaStreamCaptureStatus cs;
   EDP_TRY(cudaStreamIsCapturing(p->stream, &cs));
   if (cs != cudaStreamCaptureStatusActive) return EDP_ERR_STATE;
-  return enqueue_events(p, p->stream, true);
+  return enqueue(p, p->stream, true);
 }
 
 int edp_capture(edp_peeler *p) {
@@ -362,7 +465,7 @@ int edp_capture(edp_peeler *p) {
     if (rc) return rc;
   }
   EDP_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_events(p, p->stream, true);
+  int rc = enqueue(p, p->stream, true);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(p->stream, &g);
   if (rc) {
@@ -422,6 +525,7 @@ void edp_destroy(edp_peeler *p) {
   tree_free(p->source_tree);
   tree_free(p->seg_tree);
   tree_free(p->point_tree);
+  tree_free(p->residual_tree);
   for (void *a : p->allocations) cudaFree(a);
   if (p->body_stream) cudaStreamDestroy(p->body_stream);
   for (auto &e : p->stage_exec)
@@ -449,7 +553,7 @@ int edp_run_stage(edp_peeler *p, int32_t stage) {
     EDP_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     if (stage == 0) {
-      e = stage_prepare(d, p->scratch, p->source_tree, p->seg_tree, p->stream);
+      e = run_prepare(p, d, p->stream);
     } else if (stage == 1) {
       e = stage_mesh_index(d, p->scratch, p->point_tree, p->stream);
     } else {
