@@ -260,6 +260,58 @@ def separated_any(a, b) -> bool:
     return False
 
 
+def project_triangle(cam, window, camv):
+    """Near clip, projection, depth-plane fit and window clip of one triangle
+    given in exact camera coordinates (camera.cpp:108-154).
+
+    Returns (score, ccw polygon, projected points, in_window), or the reason it
+    is dropped: "clipped_empty" or "zero_area"."""
+    xmin, ymin, xmax, ymax = window
+    clipped = list(camv)
+    if cam.perspective:
+        clipped = []
+        for i in range(3):
+            a, b = camv[i], camv[(i + 1) % 3]
+            da, db = a[2] - cam.near, b[2] - cam.near
+            if da >= 0:
+                clipped.append(a)
+            if (da < 0 and db > 0) or (da > 0 and db < 0):
+                u = da / (da - db)
+                clipped.append(tuple(a[k] + (b[k] - a[k]) * u for k in range(3)))
+    if len(clipped) < 3:
+        return "clipped_empty"
+    projected, depths = [], []
+    for p in clipped:
+        if cam.perspective:
+            projected.append((p[0] / p[2], p[1] / p[2]))
+            depths.append(-Q(1) / p[2])
+        else:
+            projected.append((p[0], p[1]))
+            depths.append(p[2])
+    k = 2
+    while k < len(projected) and collinear(projected[0], projected[1], projected[k]):
+        k += 1
+    if k == len(projected):
+        return "zero_area"
+    score = fit([projected[0], projected[1], projected[k]], [depths[0], depths[1], depths[k]])
+    in_window = all(xmin <= p[0] <= xmax and ymin <= p[1] <= ymax for p in projected)
+    poly = polygon(projected)
+    if not in_window and poly:
+        for f in (
+            lambda p: p[0] - xmin,
+            lambda p: xmax - p[0],
+            lambda p: p[1] - ymin,
+            lambda p: ymax - p[1],
+        ):
+            poly = clip_halfplane(poly, f)
+            if not poly:
+                break
+        poly = polygon(poly)
+    if not poly:
+        return "clipped_empty"
+    return score, poly, projected, in_window
+
+
 def read_scene(data, resolved_mesh=True) -> Scene:
     """Exact scene import; ``data`` is the parsed scene JSON (or a path)."""
     if isinstance(data, (str, Path)):
@@ -293,53 +345,14 @@ def read_scene(data, resolved_mesh=True) -> Scene:
             pw = tuple(rational(x) for x in v)
             world.append(pw)
             camv.append(transform(cam.world_to_camera, pw))
-        clipped = list(camv)
-        if cam.perspective:
-            clipped = []
-            for i in range(3):
-                a, b = camv[i], camv[(i + 1) % 3]
-                da, db = a[2] - cam.near, b[2] - cam.near
-                if da >= 0:
-                    clipped.append(a)
-                if (da < 0 and db > 0) or (da > 0 and db < 0):
-                    u = da / (da - db)
-                    clipped.append(tuple(a[k] + (b[k] - a[k]) * u for k in range(3)))
-        if len(clipped) < 3:
-            s.clipped_empty += 1
-            continue
-        projected, depths = [], []
-        for p in clipped:
-            if cam.perspective:
-                projected.append((p[0] / p[2], p[1] / p[2]))
-                depths.append(-Q(1) / p[2])
+        projected_source = project_triangle(cam, window, camv)
+        if isinstance(projected_source, str):
+            if projected_source == "zero_area":
+                s.zero_area += 1
             else:
-                projected.append((p[0], p[1]))
-                depths.append(p[2])
-        k = 2
-        while k < len(projected) and collinear(projected[0], projected[1], projected[k]):
-            k += 1
-        if k == len(projected):
-            s.zero_area += 1
+                s.clipped_empty += 1
             continue
-        score = fit(
-            [projected[0], projected[1], projected[k]], [depths[0], depths[1], depths[k]]
-        )
-        in_window = all(xmin <= p[0] <= xmax and ymin <= p[1] <= ymax for p in projected)
-        poly = polygon(projected)
-        if not in_window and poly:
-            for f in (
-                lambda p: p[0] - xmin,
-                lambda p: xmax - p[0],
-                lambda p: p[1] - ymin,
-                lambda p: ymax - p[1],
-            ):
-                poly = clip_halfplane(poly, f)
-                if not poly:
-                    break
-            poly = polygon(poly)
-        if not poly:
-            s.clipped_empty += 1
-            continue
+        score, poly, projected, in_window = projected_source
         clipped_camera = not in_window or (
             cam.perspective and any(v[2] < cam.near for v in camv)
         )
@@ -716,6 +729,121 @@ class RankIndex:
 
 
 def to_window(scene, u, v):
-    """Exact camera-projected point of normalised window coordinates (u, v)."""
+    """Exact camera-projected point of normalised window coordinates (u, v);
+    ``u``, ``v`` are floats (taken exactly) or Fractions."""
     xmin, ymin, xmax, ymax = scene.window
     return (xmin + Q(u) * (xmax - xmin), ymin + Q(v) * (ymax - ymin))
+
+
+class SparseRanks:
+    """Exact ranks on large meshes: source triangles are imported exactly only
+    when a query point needs them.
+
+    The inputs are the device arrays themselves (binary64 vertices, int faces,
+    a 4x4 affine camera, the six window/camera settings); the exact scene is
+    the rational value of every double.  Candidate sources for a point come
+    from a grid over float bounding boxes of the projected triangles, padded
+    so that no source containing the point is missed; every decision is then
+    exact (the same predicates as ``RankIndex``)."""
+
+    def __init__(self, vertices, faces, camera, settings, cells=512):
+        import numpy as np
+
+        self.vertices = np.asarray(vertices, dtype=np.float64)
+        self.faces = np.asarray(faces, dtype=np.int64)
+        camera = np.asarray(camera, dtype=np.float64).reshape(4, 4)
+        settings = np.asarray(settings, dtype=np.float64)
+        self.cam = Camera(perspective=bool(settings[4] != 0), near=Q(float(settings[5])),
+                          world_to_camera=[[Q(float(x)) for x in camera[r]] for r in range(3)])
+        self.window = tuple(Q(float(x)) for x in settings[:4])
+        self.cache: dict = {}
+        # Float projection, conservative boxes in normalised window coordinates.
+        cam = self.vertices @ camera[:3, :3].T + camera[:3, 3]
+        tri = cam[self.faces]  # [N, 3, 3]
+        w = settings
+        scale = np.array([w[2] - w[0], w[3] - w[1]])
+        if settings[4]:
+            z = tri[:, :, 2]
+            front = (z > w[5]).all(axis=1)
+            xy = tri[:, :, :2] / np.where(z > 0, z, 1.0)[:, :, None]
+        else:
+            front = np.ones(len(tri), bool)
+            xy = tri[:, :, :2]
+        uv = (xy - w[:2]) / scale
+        lo, hi = uv.min(axis=1), uv.max(axis=1)
+        pad = 1e-9 * (1.0 + np.abs(lo).max(axis=1, initial=0) + np.abs(hi).max(axis=1, initial=0))
+        lo = lo - pad[:, None]
+        hi = hi + pad[:, None]
+        # Triangles crossing the near plane: their projection is unbounded; every
+        # query must consider them.
+        self.always = np.nonzero(~front)[0].tolist()
+        self.cells = cells
+        clo = np.clip(np.floor(lo * cells), 0, cells - 1).astype(np.int64)
+        chi = np.clip(np.floor(hi * cells), 0, cells - 1).astype(np.int64)
+        self.grid: dict = {}
+        self.lo, self.hi = lo, hi
+        for f in np.nonzero(front)[0]:
+            for cx in range(clo[f, 0], chi[f, 0] + 1):
+                for cy in range(clo[f, 1], chi[f, 1] + 1):
+                    self.grid.setdefault((cx, cy), []).append(int(f))
+
+    def source(self, f):
+        """(score, exact ccw polygon) of face f, or None if it projects to nothing."""
+        if f not in self.cache:
+            camv = []
+            for v in self.faces[f]:
+                pw = tuple(Q(float(x)) for x in self.vertices[v])
+                camv.append(transform(self.cam.world_to_camera, pw))
+            got = project_triangle(self.cam, self.window, camv)
+            self.cache[f] = None if isinstance(got, str) else (got[0], got[1])
+        return self.cache[f]
+
+    def candidates(self, u, v):
+        cx = min(self.cells - 1, max(0, int(u * self.cells)))
+        cy = min(self.cells - 1, max(0, int(v * self.cells)))
+        out = [f for f in self.grid.get((cx, cy), [])
+               if self.lo[f, 0] <= u <= self.hi[f, 0] and self.lo[f, 1] <= v <= self.hi[f, 1]]
+        return out + self.always
+
+    def rank(self, face, u, v):
+        """Exact rank of `face` at normalised window point (u, v); None if ambiguous."""
+        src = self.source(face)
+        if src is None:
+            return None
+        p = to_window(self, u, v)
+        if strictly_inside(src[1], p) != 1:
+            return None
+        z = src[0].at(p)
+        rank = 0
+        for j in self.candidates(u, v):
+            if j == face:
+                continue
+            other = self.source(j)
+            if other is None:
+                continue
+            inside = strictly_inside(other[1], p)
+            if inside < 0:
+                continue
+            if inside == 0:
+                return None
+            zj = other[0].at(p)
+            if zj == z:
+                return None
+            rank += zj < z
+        return rank
+
+    def polygon_rank(self, face, ring):
+        """First unambiguous exact rank at generic interior points of a
+        normalised-coordinate ring (vertex mean, then blends toward vertices)."""
+        n = len(ring)
+        cu = sum(Q(float(x)) for x, _ in ring) / n
+        cv = sum(Q(float(y)) for _, y in ring) / n
+        points = [(cu, cv)]
+        for w in (Q(1, 3), Q(1, 7), Q(2, 5)):
+            for x, y in ring:
+                points.append((cu + w * (Q(float(x)) - cu), cv + w * (Q(float(y)) - cv)))
+        for u, v in points:
+            r = self.rank(face, u, v)
+            if r is not None:
+                return r
+        return None
