@@ -142,6 +142,9 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
       params[m + 1] = v;
     }
     // Count this edge's fan triangles, reserve their slots at once, then emit.
+    // A triangle is emitted only when its signed doubled area exceeds EPS^2:
+    // noded points 1e-13 apart can otherwise give slivers of area ~1e-19 whose
+    // orientation rounding decides (the reference tests |area|, kernels.py:1105).
     int emitted = 0;
     {
       double previous = 0.0;
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
         double following = step < count ? params[step] : 1.0;
         if (following <= previous + kEps) continue;
         V2 next = a + following * dir;
-        if (fabs(cross(center, cursor, next)) > kEps * kEps) ++emitted;
+        if (cross(center, cursor, next) > kEps * kEps) ++emitted;
         cursor = next;
         previous = following;
       }
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
       V2 next = a + following * dir;
       double w_next[3];
       lift(d, next, sc, w_next);
-      if (fabs(cross(center, cursor, next)) > kEps * kEps) {
+      if (cross(center, cursor, next) > kEps * kEps) {
         V2 *uv = d.tri_uv + 3 * int64_t(slot);
         double *w = d.tri_world + 9 * int64_t(slot);
         uv[0] = center;
