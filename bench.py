@@ -40,6 +40,8 @@ def workload_config(name, vertices, faces):
                       "0.3 with N(0,0.02) noise (seed 2), pinhole 60 deg at 3x bounding radius",
         "icospheres-2560": "two nested noisy icospheres, 2 x 1,280 faces, orthographic",
         "stack-65536": "65,536 identical-footprint triangles at z = i*1e-3, orthographic",
+        "primitives-720k": "40 noisy spheres and tori (radii log-uniform in [0.05, 0.5], seed 7) "
+                           "packed disjointly, 720,916 faces, pinhole 60 deg",
     }
     return {"workload": f"{name}: {descriptions.get(name, name)}", "faces": int(len(faces)),
             "vertices": int(len(vertices)),

@@ -170,7 +170,103 @@ def stress_stack(n=65536, jitter=1e-9, seed=3):
     return vertices, faces, camera, settings
 
 
+def uv_sphere(rings, segments, radius, noise, rng):
+    """Closed noisy sphere: 2 * segments * (rings - 1) faces, outward winding."""
+    theta = np.linspace(0, np.pi, rings + 1)[1:-1]
+    phi = np.linspace(0, 2 * np.pi, segments, endpoint=False)
+    body = np.stack([np.sin(theta)[:, None] * np.cos(phi)[None],
+                     np.sin(theta)[:, None] * np.sin(phi)[None],
+                     np.cos(theta)[:, None] * np.ones_like(phi)[None]], -1).reshape(-1, 3)
+    vertices = np.concatenate([[[0, 0, 1]], body, [[0, 0, -1]]])
+    vertices = vertices * (radius * (1 + rng.uniform(-noise, noise, size=(len(vertices), 1))))
+    top, bottom = 0, len(vertices) - 1
+    ring = lambda i, j: 1 + i * segments + j % segments  # noqa: E731
+    faces = []
+    for j in range(segments):
+        faces.append((top, ring(0, j), ring(0, j + 1)))
+        faces.append((bottom, ring(rings - 2, j + 1), ring(rings - 2, j)))
+    for i in range(rings - 2):
+        for j in range(segments):
+            a, b, c, d = ring(i, j), ring(i + 1, j), ring(i + 1, j + 1), ring(i, j + 1)
+            faces += [(a, b, c), (a, c, d)]
+    return vertices, np.array(faces, dtype=np.int32)
+
+
+def torus(major_segments, minor_segments, major, minor, noise, rng):
+    """Closed noisy torus: 2 * major_segments * minor_segments faces."""
+    u = np.linspace(0, 2 * np.pi, major_segments, endpoint=False)[:, None]
+    v = np.linspace(0, 2 * np.pi, minor_segments, endpoint=False)[None, :]
+    r = minor * (1 + rng.uniform(-noise, noise, size=(major_segments, minor_segments)))
+    vertices = np.stack([(major + r * np.cos(v)) * np.cos(u), (major + r * np.cos(v)) * np.sin(u),
+                         r * np.sin(v)], -1).reshape(-1, 3)
+    i = np.arange(major_segments)[:, None]
+    j = np.arange(minor_segments)[None, :]
+    a = i * minor_segments + j
+    b = ((i + 1) % major_segments) * minor_segments + j
+    c = ((i + 1) % major_segments) * minor_segments + (j + 1) % minor_segments
+    d = i * minor_segments + (j + 1) % minor_segments
+    faces = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3),
+                            np.stack([a, c, d], -1).reshape(-1, 3)]).astype(np.int32)
+    return vertices, faces
+
+
+def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7):
+    """``count`` noisy spheres and tori (bounding radii log-uniform in
+    [0.05, 0.5], faces in proportion to surface area, about ``total_faces`` in
+    all), placed without overlap by rejection sampling in a cube that grows
+    until they fit, then viewed by a 60 degree pinhole camera at 3x the scene's
+    bounding radius.  Disjoint placement stands in for resolving overlapping
+    primitives, which needs an exact mesh-intersection resolver."""
+    rng = np.random.default_rng(seed)
+    radii = np.exp(rng.uniform(np.log(0.05), np.log(0.5), size=count))
+    kinds = rng.integers(0, 2, size=count)  # 0 sphere, 1 torus
+    area = np.where(kinds == 0, 4 * np.pi * radii ** 2, 4 * np.pi ** 2 * (0.7 * radii) * (0.3 * radii))
+    budget = total_faces * area / area.sum()
+    side, centers = 1.0, []
+    while len(centers) < count:
+        centers = []
+        for r in radii:
+            for _ in range(2000):
+                c = rng.uniform(r, side - r, size=3)
+                if all(np.linalg.norm(c - c2) > r + r2 for c2, r2 in zip(centers, radii)):
+                    centers.append(c)
+                    break
+            else:
+                break
+        side *= 1.1
+    parts_v, parts_f, offset = [], [], 0
+    for r, kind, faces, c in zip(radii, kinds, budget, centers):
+        if kind == 0:
+            rings = max(3, int(round(np.sqrt(faces / 4.0))) + 1)
+            v, f = uv_sphere(rings, 2 * (rings - 1), r / (1 + noise), noise, rng)
+        else:
+            minor_segments = max(3, int(round(np.sqrt(faces / 6.0))))
+            major_segments = max(3, int(round(faces / (2 * minor_segments))))
+            v, f = torus(major_segments, minor_segments, 0.7 * r, 0.3 * r / (1 + noise), noise, rng)
+            v = v @ _random_rotation(rng).T
+        parts_v.append(v + c)
+        parts_f.append(f + offset)
+        offset += len(v)
+    vertices = np.concatenate(parts_v)
+    faces = np.concatenate(parts_f).astype(np.int32)
+    centroid = vertices.mean(0)
+    bound = np.linalg.norm(vertices - centroid, axis=1).max()
+    camera, settings = _pinhole(centroid + np.array([0.3, 0.4, 3.0]) / np.linalg.norm([0.3, 0.4, 3.0])
+                                * 3 * bound, centroid, near=0.01 * bound)
+    return vertices, faces, camera, settings
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
 CONFIGS = {
+    "primitives-720k": packed_primitives,
     "icospheres-2560": nested_icospheres,
     "knot-65536": knot_tube,
     "stack-65536": lambda: stress_stack(65536, 0.0),
