@@ -270,7 +270,7 @@ def run_ours(args, rank, world, local_rank):
     emit_bytes = 128 * check["triangles"] + 16 * check["boundary_vertices"] + 32 * check["polygons"]
     emit_ms = float(stage_ms["mesh_emit"])
     roofline = {
-        "bound": "hbm", "kernel": "k_mesh_edges (noding, fan emission, world lift)",
+        "bound": "hbm", "kernel": "k_mesh_polygons (noding, fan emission, world lift)",
         "achieved": emit_bytes / (emit_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
         "frac": emit_bytes / (emit_ms * 1e-3) / 1e9 / peak, "traffic": None,
         "peak_source": f"{peak_kind} copy bandwidth", "algorithmic_bytes": emit_bytes,

@@ -168,7 +168,6 @@ struct Dev {
   int *point_table;
   int point_mask;
   float4 *pt_lo, *pt_hi;
-  int2 *mtasks;
   V2 *tri_uv;        // [triangles][3]
   double *tri_world; // [triangles][3][3]
   int *tri_src, *tri_layer;

@@ -37,15 +37,17 @@ __global__ void k_scatter(Dev d) {
   for (int64_t i = tid(); i < live; i += stride()) {
     if (d.status[kError] != 0) return;
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
-    const int n = d.out_n[i], layer = d.out_layer[i];
+    const int layer = d.out_layer[i];
+    const int64_t base = d.offsets[i];
+    const int n = int(min(int64_t(d.out_n[i]), d.cap.vertices - base));
     for (int j = 0; j < n; ++j) {
-      int64_t slot = int64_t(d.offsets[i]) + j;
-      if (slot >= d.cap.vertices) break;
-      V2 x = p[j];
-      d.bverts[slot] = x;
-      d.blayers[slot] = layer;
-      d.mtasks[slot] = make_int2(int(i), j);
-      __threadfence();  // publish the point before its slot can be found in the table
+      d.bverts[base + j] = p[j];
+      d.blayers[base + j] = layer;
+    }
+    __threadfence();  // publish the points before their slots can be found in the table
+    for (int j = 0; j < n; ++j) {
+      const int64_t slot = base + j;
+      const V2 x = p[j];
       uint64_t h = mix64(mix64(key_bits(x.x)) ^ key_bits(x.y)) ^ mix64(uint64_t(layer) + 7ull);
       uint32_t probe = uint32_t(h) & uint32_t(d.point_mask);
       bool fresh = false;
@@ -85,45 +87,58 @@ __device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
   for (int r = 0; r < 3; ++r) w[r] = m[4 * r] * u + m[4 * r + 1] * v + m[4 * r + 2] * z + m[4 * r + 3];
 }
 
-// Node one polygon edge against every same-layer boundary vertex lying on it
-// (collinear within EPS, strictly inside the edge), sort the split
-// parameters, and emit centroid-fan triangles lifted to world space
-// (kernels.py:1009-1125).
-__global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity) {
-  const int tasks = d.sc[kLiveVertices];
+// Node every edge of one output polygon against the same-layer boundary
+// vertices lying on it (collinear within EPS, strictly inside the edge), then
+// emit the polygon's centroid fan with the split points, lifted to world
+// space (kernels.py:1009-1125).  One point-hierarchy query per polygon (its
+// box contains every edge's box) replaces the reference's query per edge; the
+// acceptance test and therefore the triangles are the same.
+constexpr int kPolygonSplits = 256;  // split points buffered per polygon
+
+__global__ void __launch_bounds__(kBlock) k_mesh_polygons(Dev d, int edge_capacity) {
+  const int live = d.sc[kLivePolygons];
   const int leaves = *d.point_tree.size;
-  double params[kMaxEdgeVertices];
-  for (int64_t t = tid(); t < tasks; t += stride()) {
+  double split_t[kPolygonSplits];
+  unsigned char split_edge[kPolygonSplits];
+  for (int64_t i = tid(); i < live; i += stride()) {
     if (d.status[kError] != 0) return;
-    const int2 task = d.mtasks[t];
-    const int i = task.x, edge = task.y;
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
     const int n = d.out_n[i];
-    if (edge >= n) continue;
+    if (n < 3) continue;
     const int layer = d.out_layer[i], source = d.out_src[i];
-    V2 a = p[edge], b = p[(edge + 1) % n], dir = b - a;
-    double length2 = dot(dir, dir);
+    double lx = 1.0e30, ly = 1.0e30, hx = -1.0e30, hy = -1.0e30;
     V2 center = v2(0.0, 0.0);
-    for (int j = 0; j < n; ++j) center = center + p[j] / double(n);
-    float4 lo = make_float4(__double2float_rd(fmin(a.x, b.x) - 2.0e-7),
-                            __double2float_rd(fmin(a.y, b.y) - 2.0e-7), float(layer), 0.f);
-    float4 hi = make_float4(__double2float_ru(fmax(a.x, b.x) + 2.0e-7),
-                            __double2float_ru(fmax(a.y, b.y) + 2.0e-7), float(layer), 0.f);
-    int count = 0, node = 1;
+    for (int j = 0; j < n; ++j) {
+      lx = fmin(lx, p[j].x); ly = fmin(ly, p[j].y);
+      hx = fmax(hx, p[j].x); hy = fmax(hy, p[j].y);
+      center = center + p[j] / double(n);
+    }
+    const float4 lo = make_float4(__double2float_rd(lx - 2.0e-7), __double2float_rd(ly - 2.0e-7),
+                                  float(layer), 0.f);
+    const float4 hi = make_float4(__double2float_ru(hx + 2.0e-7), __double2float_ru(hy + 2.0e-7),
+                                  float(layer), 0.f);
+    int count = 0, per_edge[kMaxVertices];
+    for (int e = 0; e < n; ++e) per_edge[e] = 0;
     bool overflow = false;
-    const double tol = kEps * sqrt(length2);
-    while (node > 0 && length2 > 0.0) {
+    int node = 1;
+    while (node > 0 && !overflow) {
       int j;
       node = query_next(d.point_tree, leaves, lo, hi, node, 0, j);
       if (j < 0) break;
-      V2 x = d.uverts[j];
-      double tt = dot(x - a, dir) / length2;
-      if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= tol) {
-        if (count < edge_capacity) {
-          params[count++] = tt;
-        } else {
-          overflow = true;
-          break;
+      const V2 x = d.uverts[j];
+      for (int e = 0; e < n; ++e) {
+        const V2 a = p[e], b = p[(e + 1) % n], dir = b - a;
+        const double length2 = dot(dir, dir);
+        if (!(length2 > 0.0)) continue;
+        const double tt = dot(x - a, dir) / length2;
+        if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= kEps * sqrt(length2)) {
+          if (++per_edge[e] > edge_capacity || count == kPolygonSplits) {
+            overflow = true;
+            break;
+          }
+          split_t[count] = tt;
+          split_edge[count] = (unsigned char)e;
+          ++count;
         }
       }
     }
@@ -131,31 +146,38 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
       set_error(d.status, kErrEdgeNoding);
       return;
     }
-    // Insertion sort: edges carry few split points; the bound is edge_capacity.
+    // Order the split points by (edge, parameter).
     for (int k = 1; k < count; ++k) {
-      double v = params[k];
+      const double t = split_t[k];
+      const unsigned char e = split_edge[k];
       int m = k - 1;
-      while (m >= 0 && params[m] > v) {
-        params[m + 1] = params[m];
+      while (m >= 0 && (split_edge[m] > e || (split_edge[m] == e && split_t[m] > t))) {
+        split_t[m + 1] = split_t[m];
+        split_edge[m + 1] = split_edge[m];
         --m;
       }
-      params[m + 1] = v;
+      split_t[m + 1] = t;
+      split_edge[m + 1] = e;
     }
-    // Count this edge's fan triangles, reserve their slots at once, then emit.
-    // A triangle is emitted only when its signed doubled area exceeds EPS^2:
-    // noded points 1e-13 apart can otherwise give slivers of area ~1e-19 whose
-    // orientation rounding decides (the reference tests |area|, kernels.py:1105).
+    // Count the fan triangles (signed doubled area above EPS^2: noded points
+    // 1e-13 apart can otherwise give slivers of area ~1e-19 whose orientation
+    // rounding decides; the reference tests |area|, kernels.py:1105), reserve
+    // their slots at once, then emit.
     int emitted = 0;
-    {
+    for (int e = 0, k = 0; e < n; ++e) {
+      const V2 a = p[e], dir = p[(e + 1) % n] - a;
       double previous = 0.0;
       V2 cursor = a;
-      for (int step = 0; step <= count; ++step) {
-        double following = step < count ? params[step] : 1.0;
-        if (following <= previous + kEps) continue;
-        V2 next = a + following * dir;
-        if (cross(center, cursor, next) > kEps * kEps) ++emitted;
-        cursor = next;
-        previous = following;
+      for (;;) {
+        const bool last = !(k < count && split_edge[k] == e);
+        const double following = last ? 1.0 : split_t[k++];
+        if (following > previous + kEps) {
+          const V2 next = a + following * dir;
+          if (cross(center, cursor, next) > kEps * kEps) ++emitted;
+          cursor = next;
+          previous = following;
+        }
+        if (last) break;
       }
     }
     int slot = reserve(&d.status[kTriangles], emitted);
@@ -166,34 +188,40 @@ __global__ void __launch_bounds__(kBlock) k_mesh_edges(Dev d, int edge_capacity)
     const Plane sc = d.scores[source];
     double w_center[3];
     lift(d, center, sc, w_center);
-    double previous = 0.0;
-    V2 cursor = a;
-    double w_cursor[3];
-    lift(d, cursor, sc, w_cursor);
-    for (int step = 0; step <= count; ++step) {
-      double following = step < count ? params[step] : 1.0;
-      if (following <= previous + kEps) continue;
-      V2 next = a + following * dir;
-      double w_next[3];
-      lift(d, next, sc, w_next);
-      if (cross(center, cursor, next) > kEps * kEps) {
-        V2 *uv = d.tri_uv + 3 * int64_t(slot);
-        double *w = d.tri_world + 9 * int64_t(slot);
-        uv[0] = center;
-        uv[1] = cursor;
-        uv[2] = next;
-        for (int k = 0; k < 3; ++k) {
-          w[k] = w_center[k];
-          w[3 + k] = w_cursor[k];
-          w[6 + k] = w_next[k];
+    for (int e = 0, k = 0; e < n; ++e) {
+      const V2 a = p[e], dir = p[(e + 1) % n] - a;
+      double previous = 0.0;
+      V2 cursor = a;
+      double w_cursor[3];
+      lift(d, cursor, sc, w_cursor);
+      for (;;) {
+        const bool last = !(k < count && split_edge[k] == e);
+        const double following = last ? 1.0 : split_t[k++];
+        if (following > previous + kEps) {
+          const V2 next = a + following * dir;
+          double w_next[3];
+          lift(d, next, sc, w_next);
+          if (cross(center, cursor, next) > kEps * kEps) {
+            V2 *uv = d.tri_uv + 3 * int64_t(slot);
+            double *w = d.tri_world + 9 * int64_t(slot);
+            uv[0] = center;
+            uv[1] = cursor;
+            uv[2] = next;
+            for (int c = 0; c < 3; ++c) {
+              w[c] = w_center[c];
+              w[3 + c] = w_cursor[c];
+              w[6 + c] = w_next[c];
+            }
+            d.tri_src[slot] = source;
+            d.tri_layer[slot] = layer;
+            ++slot;
+          }
+          cursor = next;
+          for (int c = 0; c < 3; ++c) w_cursor[c] = w_next[c];
+          previous = following;
         }
-        d.tri_src[slot] = source;
-        d.tri_layer[slot] = layer;
-        ++slot;
+        if (last) break;
       }
-      cursor = next;
-      for (int k = 0; k < 3; ++k) w_cursor[k] = w_next[k];
-      previous = following;
     }
   }
 }
@@ -222,7 +250,7 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
 
 cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st) {
   int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
-  k_mesh_edges<<<blocks(d.cap.vertices), kBlock, 0, st>>>(d, cap);
+  k_mesh_polygons<<<blocks(d.cap.regions), kBlock, 0, st>>>(d, cap);
   note_launch();
   return cudaGetLastError();
 }

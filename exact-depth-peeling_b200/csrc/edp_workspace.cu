@@ -119,7 +119,6 @@ cudaError_t allocate_shared(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
   EDP_CHECK(alloc(p, &d.pt_lo, E));
   EDP_CHECK(alloc(p, &d.pt_hi, E));
-  EDP_CHECK(alloc(p, &d.mtasks, E));
   EDP_CHECK(alloc(p, &d.tri_uv, 3 * T));
   EDP_CHECK(alloc(p, &d.tri_world, 9 * T));
   EDP_CHECK(alloc(p, &d.tri_src, T));
