@@ -130,6 +130,10 @@ __global__ void __launch_bounds__(kBlock) k_mesh_polygons(Dev d, int edge_capaci
         const V2 a = p[e], b = p[(e + 1) % n], dir = b - a;
         const double length2 = dot(dir, dir);
         if (!(length2 > 0.0)) continue;
+        // Division-free rejection of points off the edge's line (4x slack over
+        // the exact test below, which alone decides).
+        const double off = cross(a, b, x);
+        if (off * off > 4.0 * kEps * kEps * length2) continue;
         const double tt = dot(x - a, dir) / length2;
         if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= kEps * sqrt(length2)) {
           if (++per_edge[e] > edge_capacity || count == kPolygonSplits) {
