@@ -27,36 +27,15 @@ __device__ inline bool front_segment(const V2 *p, int n, V2 a, V2 b, double za, 
   return high > low;
 }
 
-// Resident threads of a B200 (148 SMs x 2048): while fewer patches than this
-// remain, each may test proportionally more candidates per round.
-constexpr int kResidentThreads = 148 * 2048;
-constexpr int kMaxBudget = 4096;
-
-__device__ inline void push(const Dev &d, V2 *nv, int *nn, int *nsrc, int *ncur, const V2 *p,
-                            int n, int source, int node) {
-  const int slot = reserve(&d.status[kNextResidual], 1);
-  if (slot >= d.cap.frontier) {
-    set_error(d.status, kErrResidual);
-    return;
-  }
-  V2 *dst = nv + int64_t(kMaxVertices) * slot;
-  for (int j = 0; j < n; ++j) dst[j] = p[j];
-  nn[slot] = n;
-  nsrc[slot] = source;
-  ncur[slot] = node;
-}
-
-// One frontier round (frontier.py:106-223).  A patch walks the contour-segment
-// hierarchy from its cursor.  The first segment that crosses the patch
-// interior and is nearer somewhere splits it along the segment's supporting
-// line; a patch whose walk completes is final and goes to the output pool.
-// Differences from the reference's schedule, which leave every patch's fate
-// unchanged: after a split the thread continues at once with the left child
-// (from the same cursor) and only the right child waits for the next round;
-// and the per-round candidate budget grows as the frontier shrinks (32 per
-// patch when the GPU is full, up to kMaxBudget), so long contour walks need
-// far fewer rounds.
+// One frontier round.  Each patch visits at most kCandidatesPerPass contour
+// segments of the segment hierarchy, continuing from its cursor.  The first
+// segment that crosses the patch interior and is nearer somewhere splits the
+// patch along its supporting line into two next-round patches that inherit the
+// cursor; a patch whose traversal completes is final and goes to the output
+// pool; otherwise it carries over (frontier.py:106-223).  Slots are reserved
+// once per converged group of threads and counters are flushed once per thread.
 __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
+  enum Action { kSkip = 0, kSplit = 1, kCarry = 2, kDone = 3 };
   const int par = *d.parity;
   const V2 *fv = d.fv[par];
   const int *fn = d.fn[par], *fsrc = d.fsrc[par], *fcur = d.fcur[par];
@@ -64,102 +43,113 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
   int *nn = d.fn[par ^ 1], *nsrc = d.fsrc[par ^ 1], *ncur = d.fcur[par ^ 1];
   const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
   const int leaves = *d.seg_tree.size;
-  const int budget = live >= kResidentThreads / kCandidatesPerPass
-                         ? kCandidatesPerPass
-                         : int(min(int64_t(kMaxBudget),
-                                   int64_t(kResidentThreads) / max(live, 1)));
   long long visits = 0, tests = 0, splits = 0;
-  V2 cur[kMaxVertices], left_v[kMaxVertices], right_v[kMaxVertices];
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < live;
        i += int64_t(gridDim.x) * blockDim.x) {
     if (d.status[kError] != 0) return;
-    int n = fn[i];
+    const int n = fn[i];
     if (n == 0) continue;
     ++visits;
     const int source = fsrc[i];
     int node = fcur[i];
-    {
-      const V2 *p = fv + int64_t(kMaxVertices) * i;
-      for (int j = 0; j < n; ++j) cur[j] = p[j];
-    }
+    const V2 *p = fv + int64_t(kMaxVertices) * i;
     const Plane sc = d.scores[source];
-    int left_budget = budget;
-    while (true) {
-      float4 lo, hi;
-      polygon_bounds(cur, n, sc, lo, hi);
-      lo.z = -1.0e30f;
-      bool done = false, split = false;
-      V2 a = v2(0.0, 0.0), b = a;
-      while (left_budget > 0) {
-        int c;
-        node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
-        if (c < 0) {
-          done = true;
-          break;
-        }
-        --left_budget;
-        ++tests;
-        a = d.seg_a[c];
-        b = d.seg_b[c];
-        bool positive = false, negative = false;
-        for (int j = 0; j < n; ++j) {
-          double side = cross(a, b, cur[j]);
-          positive |= side > 0.0;
-          negative |= side < 0.0;
-        }
-        if (!(positive && negative)) continue;
-        const V2 near = d.seg_near[c];
-        double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
-        if (front_segment(cur, n, a, b, za, zb)) {
-          split = true;
-          break;
-        }
-      }
-      if (done) {
-        const int out = reserve(&d.status[kPolygons], 1);
-        if (out >= d.cap.regions) {
-          set_error(d.status, kErrOutput);
-          break;
-        }
-        V2 *dst = d.out_v + int64_t(kMaxVertices) * out;
-        for (int j = 0; j < n; ++j) dst[j] = cur[j];
-        d.out_n[out] = n;
-        d.out_src[out] = source;
-        d.out_layer[out] = 0;
+    float4 lo, hi;
+    polygon_bounds(p, n, sc, lo, hi);
+    lo.z = -1.0e30f;
+    int action = kCarry;
+    V2 a = v2(0.0, 0.0), b = a;
+    for (int task = 0; task < kCandidatesPerPass; ++task) {
+      int c;
+      node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
+      if (c < 0) {
+        action = kDone;
         break;
       }
-      if (!split) {  // budget spent: carry the patch and its cursor over
-        push(d, nv, nn, nsrc, ncur, cur, n, source, node);
-        break;
-      }
-      int left = 0, right = 0;
-      const V2 dir = b - a;
-      const Plane s{-dir.y, dir.x, 0.0, 0.0};
+      ++tests;
+      a = d.seg_a[c];
+      b = d.seg_b[c];
+      bool positive = false, negative = false;
       for (int j = 0; j < n; ++j) {
-        V2 u = cur[j], v = cur[(j + 1) % n];
-        double du = value(s, u - a), dv = value(s, v - a);
-        if (du >= 0.0) left = append(left_v, left, u);
-        if (du <= 0.0) right = append(right_v, right, u);
-        if ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0)) {
-          V2 x = u + (du / (du - dv)) * (v - u);
-          left = append(left_v, left, x);
-          right = append(right_v, right, x);
-        }
+        double side = cross(a, b, p[j]);
+        positive |= side > 0.0;
+        negative |= side < 0.0;
       }
-      left = clean(left_v, left);
-      right = clean(right_v, right);
-      if (left > kMaxVertices || right > kMaxVertices) {
-        set_error(d.status, kErrPolygon);
+      if (!(positive && negative)) continue;
+      const V2 near = d.seg_near[c];
+      double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
+      if (front_segment(p, n, a, b, za, zb)) {
+        action = kSplit;
         break;
       }
-      if (left > 0 && right > 0) {
-        ++splits;
-        push(d, nv, nn, nsrc, ncur, right_v, right, source, node);
-        for (int j = 0; j < left; ++j) cur[j] = left_v[j];
-        n = left;
-      }
-      // A collapsed child cancels the cut; the parent continues past it.
     }
+    const int slot = reserve(&d.status[kNextResidual],
+                             action == kSplit ? 2 : action == kCarry ? 1 : 0);
+    const int out = reserve(&d.status[kPolygons], action == kDone ? 1 : 0);
+    if (action == kDone) {
+      if (out >= d.cap.regions) {
+        set_error(d.status, kErrOutput);
+        continue;
+      }
+      V2 *dst = d.out_v + int64_t(kMaxVertices) * out;
+      for (int j = 0; j < n; ++j) dst[j] = p[j];
+      d.out_n[out] = n;
+      d.out_src[out] = source;
+      d.out_layer[out] = 0;
+      continue;
+    }
+    if (action == kCarry) {
+      if (slot >= d.cap.frontier) {
+        set_error(d.status, kErrResidual);
+        continue;
+      }
+      V2 *dst = nv + int64_t(kMaxVertices) * slot;
+      for (int j = 0; j < n; ++j) dst[j] = p[j];
+      nn[slot] = n;
+      nsrc[slot] = source;
+      ncur[slot] = node;
+      continue;
+    }
+    if (int64_t(slot) + 1 >= d.cap.frontier) {
+      set_error(d.status, kErrResidual);
+      continue;
+    }
+    V2 *left_v = nv + int64_t(kMaxVertices) * slot;
+    V2 *right_v = left_v + kMaxVertices;
+    int left = 0, right = 0;
+    V2 dir = b - a;
+    Plane s{-dir.y, dir.x, 0.0, 0.0};
+    for (int j = 0; j < n; ++j) {
+      V2 u = p[j], v = p[(j + 1) % n];
+      double du = value(s, u - a), dv = value(s, v - a);
+      if (du >= 0.0) left = append(left_v, left, u);
+      if (du <= 0.0) right = append(right_v, right, u);
+      if ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0)) {
+        V2 x = u + (du / (du - dv)) * (v - u);
+        left = append(left_v, left, x);
+        right = append(right_v, right, x);
+      }
+    }
+    left = clean(left_v, left);
+    right = clean(right_v, right);
+    if (left > kMaxVertices || right > kMaxVertices) {
+      set_error(d.status, kErrPolygon);
+      continue;
+    }
+    if (left > 0 && right > 0) {
+      ++splits;
+    } else {
+      // A collapsed child cancels this cut; the parent continues next round.
+      left = n;
+      right = 0;
+      for (int j = 0; j < n; ++j) left_v[j] = p[j];
+    }
+    nn[slot] = left;
+    nn[slot + 1] = right;
+    nsrc[slot] = source;
+    nsrc[slot + 1] = source;
+    ncur[slot] = node;
+    ncur[slot + 1] = node;
   }
   count_add(&d.metrics[kTargetVisits], visits);
   count_add(&d.metrics[kContourTests], tests);
