@@ -285,7 +285,8 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(args.config, vertices, faces),
         "roofline": roofline, "cpu_baseline": cpu,
-        "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": e2e_ms if e2e_steps else None, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h_bytes)},
         "gpu_launches": None, "clocks": clocks.summary(),
         "stages_ms": stage_ms,

@@ -159,12 +159,12 @@ __device__ inline void polygon_bounds(const V2 *p, int n, const Plane &score, fl
 // ---------------------------------------------------------------- hierarchy
 // A complete binary tree over a power-of-two number of Morton-ordered leaves,
 // one item per leaf; node 1 is the root, node i has children 2i and 2i+1 and
-// leaves are nodes [size, 2 size).  The size lives in device memory so one
+// leaves are nodes [size, 2 size).  A node's two corners share one 32-byte
+// sector and siblings are adjacent, so a traversal step costs one miss.  The size lives in device memory so one
 // captured graph serves any leaf count up to the allocated capacity
 // (solver.py:34-89, kernels.py:24-116).
 struct Tree {
-  const float4 *lo;
-  const float4 *hi;
+  const float4 *nodes;  // node i: nodes[2i] = lower corner, nodes[2i+1] = upper corner
   const int *ids;
   const int *size;  // device scalar: number of leaves (power of two)
 };
@@ -188,7 +188,7 @@ __device__ inline int query_next(const Tree &t, int leaves, float4 lo, float4 hi
                                  int end, int &found) {
   found = -1;
   while (node > 0 && node != end) {
-    float4 a = __ldg(&t.lo[node]), b = __ldg(&t.hi[node]);
+    float4 a = __ldg(&t.nodes[2 * node]), b = __ldg(&t.nodes[2 * node + 1]);
     if (overlaps(a, b, lo, hi)) {
       if (node < leaves) {
         node = 2 * node;

@@ -59,13 +59,13 @@ cudaError_t sort_pairs_u32(uint32_t *keys, uint32_t *keys_tmp, int *vals, int *v
 struct TreeBuffers {
   int64_t capacity = 0;   // items
   int64_t leaves_cap = 0; // power of two >= capacity
-  float4 *lo = nullptr, *hi = nullptr;  // [2 * leaves_cap]
+  float4 *nodes = nullptr;  // [2 * leaves_cap][2]: lower, upper corner of each node
   int *ids = nullptr, *ids_tmp = nullptr;
   uint64_t *keys = nullptr, *keys_tmp = nullptr;
-  int *flags = nullptr;   // [leaves_cap]
+  int *flags = nullptr;   // [1]: blocks finished in the current fit
   int *size = nullptr;    // device scalar: leaves of the current build
   int *count = nullptr;   // device scalar: items of the current build
-  Tree tree() const { return Tree{lo, hi, ids, size}; }
+  Tree tree() const { return Tree{nodes, ids, size}; }
 };
 
 cudaError_t tree_alloc(TreeBuffers &t, int64_t capacity);

@@ -265,47 +265,98 @@ __global__ void k_tree_keys(const float4 *lo, const float4 *hi, const int *count
   }
 }
 
-__global__ void k_tree_leaves(float4 *tlo, float4 *thi, const int *ids, const float4 *lo,
-                              const float4 *hi, const int *count, const int *size, int *flags) {
-  const int n = *count, leaves = *size;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < leaves;
+// Every node of a fresh hierarchy holds the empty box, which overlaps nothing.
+__global__ void k_tree_clear(float4 *nodes, int64_t count) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count;
        i += int64_t(gridDim.x) * blockDim.x) {
-    int j = ids[i];
-    float4 a = empty_lo(), b = empty_hi();
+    nodes[2 * i] = empty_lo();
+    nodes[2 * i + 1] = empty_hi();
+  }
+}
+
+__device__ inline void union_into(float4 *nodes, int node) {
+  float4 a = __ldcg(&nodes[4 * node]), c = __ldcg(&nodes[4 * node + 1]);      // child 2 node
+  float4 b = __ldcg(&nodes[4 * node + 2]), d = __ldcg(&nodes[4 * node + 3]);  // child 2 node + 1
+  __stcg(&nodes[2 * node], make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), 0.f));
+  __stcg(&nodes[2 * node + 1], make_float4(fmaxf(c.x, d.x), fmaxf(c.y, d.y), fmaxf(c.z, d.z), 0.f));
+}
+
+constexpr int kFitThreads = 256;
+constexpr int kFitLeaves = 2 * kFitThreads;  // leaves of one block's subtree
+
+// Leaves and every internal box in one launch.  Leaf i holds the box of item
+// ids[i] (the empty box past the item count).  Each block reduces whole
+// subtrees of up to kFitLeaves leaves level by level in shared memory; the
+// last block to finish then reduces the levels above the subtree roots.
+// Unions of binary32 boxes are exact, so the boxes do not depend on the order.
+__global__ void __launch_bounds__(kFitThreads)
+k_tree_fit(float4 *nodes, const int *ids, const float4 *lo, const float4 *hi, const int *count,
+           const int *size, int *done) {
+  __shared__ float4 s_lo[kFitThreads], s_hi[kFitThreads];
+  __shared__ int s_last;
+  const int n = *count, leaves = *size, t = threadIdx.x;
+  const int span = leaves < kFitLeaves ? leaves : kFitLeaves;
+  const int subtrees = leaves / span;
+  auto leaf = [&](int i, float4 &a, float4 &b) {
+    const int j = ids[i];
+    a = empty_lo();
+    b = empty_hi();
     if (j < n) {
       a = lo[j];
       b = hi[j];
     }
-    tlo[leaves + i] = a;
-    thi[leaves + i] = b;
-    flags[i] = 0;
-  }
-}
-
-__device__ inline void union_into(float4 *tlo, float4 *thi, int node) {
-  float4 a = __ldcg(&tlo[2 * node]), b = __ldcg(&tlo[2 * node + 1]);
-  float4 c = __ldcg(&thi[2 * node]), d = __ldcg(&thi[2 * node + 1]);
-  __stcg(&tlo[node], make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), 0.f));
-  __stcg(&thi[node], make_float4(fmaxf(c.x, d.x), fmaxf(c.y, d.y), fmaxf(c.z, d.z), 0.f));
-}
-
-// Bottom-up refit in one launch: the second child to finish builds its parent.
-__global__ void k_tree_refit(float4 *tlo, float4 *thi, const int *size, int *flags) {
-  const int leaves = *size, half = leaves >> 1;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < half;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    int node = half + int(i);
-    union_into(tlo, thi, node);
-    __threadfence();
-    node >>= 1;
-    while (node > 0) {
-      if (atomicAdd(&flags[node], 1) == 0) break;
-      __threadfence();
-      union_into(tlo, thi, node);
-      __threadfence();
-      node >>= 1;
+    nodes[2 * (leaves + i)] = a;
+    nodes[2 * (leaves + i) + 1] = b;
+  };
+  for (int sub = blockIdx.x; sub < subtrees; sub += gridDim.x) {
+    const int first = sub * span;
+    if (span == 1) {
+      float4 a, b;
+      if (t == 0) leaf(first, a, b);
+      continue;
+    }
+    int width = span >> 1, base = (leaves + first) >> 1;  // node id of slot 0 on this level
+    if (t < width) {
+      float4 a, b, c, e;
+      leaf(first + 2 * t, a, b);
+      leaf(first + 2 * t + 1, c, e);
+      a = make_float4(fminf(a.x, c.x), fminf(a.y, c.y), fminf(a.z, c.z), 0.f);
+      b = make_float4(fmaxf(b.x, e.x), fmaxf(b.y, e.y), fmaxf(b.z, e.z), 0.f);
+      s_lo[t] = a;
+      s_hi[t] = b;
+      nodes[2 * (base + t)] = a;
+      nodes[2 * (base + t) + 1] = b;
+    }
+    __syncthreads();
+    for (width >>= 1; width >= 1; width >>= 1) {
+      base >>= 1;
+      float4 a, b;
+      if (t < width) {
+        const float4 l0 = s_lo[2 * t], l1 = s_lo[2 * t + 1], h0 = s_hi[2 * t], h1 = s_hi[2 * t + 1];
+        a = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+        b = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+      }
+      __syncthreads();
+      if (t < width) {
+        s_lo[t] = a;
+        s_hi[t] = b;
+        nodes[2 * (base + t)] = a;
+        nodes[2 * (base + t) + 1] = b;
+      }
+      __syncthreads();
     }
   }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) s_last = atomicAdd(done, 1) == int(gridDim.x) - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int width = subtrees >> 1; width >= 1; width >>= 1) {
+    for (int k = t; k < width; k += blockDim.x) union_into(nodes, width + k);
+    __syncthreads();
+  }
+  if (t == 0) *done = 0;
 }
 
 }  // namespace
@@ -334,27 +385,37 @@ cudaError_t sort_pairs_u32(uint32_t *keys, uint32_t *keys_tmp, int *vals, int *v
   return sort_pairs<uint32_t>(keys, keys_tmp, vals, vals_tmp, count, capacity, bits, s, st);
 }
 
+cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st) {
+  const int64_t subtrees = ceil_div(t.leaves_cap, int64_t(kFitLeaves));
+  const unsigned g = unsigned(subtrees < 148 * 8 ? subtrees : 148 * 8);
+  k_tree_fit<<<g, kFitThreads, 0, st>>>(t.nodes, t.ids, lo, hi, t.count, t.size, t.flags);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t tree_alloc(TreeBuffers &t, int64_t capacity) {
   t.capacity = capacity > 0 ? capacity : 1;
   t.leaves_cap = pow2_at_least(t.capacity);
-  EDP_CHECK(cudaMalloc(&t.lo, sizeof(float4) * 2 * t.leaves_cap));
-  EDP_CHECK(cudaMalloc(&t.hi, sizeof(float4) * 2 * t.leaves_cap));
+  EDP_CHECK(cudaMalloc(&t.nodes, sizeof(float4) * 4 * t.leaves_cap));
   EDP_CHECK(cudaMalloc(&t.ids, sizeof(int) * t.leaves_cap));
   EDP_CHECK(cudaMalloc(&t.ids_tmp, sizeof(int) * t.leaves_cap));
   EDP_CHECK(cudaMalloc(&t.keys, sizeof(uint64_t) * t.leaves_cap));
   EDP_CHECK(cudaMalloc(&t.keys_tmp, sizeof(uint64_t) * t.leaves_cap));
-  EDP_CHECK(cudaMalloc(&t.flags, sizeof(int) * t.leaves_cap));
+  EDP_CHECK(cudaMalloc(&t.flags, sizeof(int)));
+  EDP_CHECK(cudaMemset(t.flags, 0, sizeof(int)));
   EDP_CHECK(cudaMalloc(&t.size, sizeof(int) * 2));
   t.count = t.size + 1;
   EDP_CHECK(cudaMemset(t.size, 0, sizeof(int) * 2));
-  // The root box of an empty tree rejects everything.
-  EDP_CHECK(cudaMemset(t.lo, 0x7f, sizeof(float4) * 2 * t.leaves_cap));
-  EDP_CHECK(cudaMemset(t.hi, 0xff, sizeof(float4) * 2 * t.leaves_cap));
+  const int64_t count = 2 * t.leaves_cap;
+  k_tree_clear<<<grid_for(count, 256) < 4 * 148 ? grid_for(count, 256) : 4 * 148, 256>>>(t.nodes, count);
+  note_launch();
+  EDP_CHECK(cudaGetLastError());
+  EDP_CHECK(cudaStreamSynchronize(0));
   return cudaSuccess;
 }
 
 void tree_free(TreeBuffers &t) {
-  cudaFree(t.lo); cudaFree(t.hi); cudaFree(t.ids); cudaFree(t.ids_tmp);
+  cudaFree(t.nodes); cudaFree(t.ids); cudaFree(t.ids_tmp);
   cudaFree(t.keys); cudaFree(t.keys_tmp); cudaFree(t.flags); cudaFree(t.size);
   t = TreeBuffers{};
 }
@@ -368,11 +429,7 @@ cudaError_t tree_build(TreeBuffers &t, const float4 *lo, const float4 *hi, const
   note_launch();
   int bits = layered ? 64 : 30;
   EDP_CHECK(sort_pairs_u64(t.keys, t.keys_tmp, t.ids, t.ids_tmp, t.count, t.leaves_cap, bits, s, st));
-  k_tree_leaves<<<g, 256, 0, st>>>(t.lo, t.hi, t.ids, lo, hi, t.count, t.size, t.flags);
-  note_launch();
-  k_tree_refit<<<g, 256, 0, st>>>(t.lo, t.hi, t.size, t.flags);
-  note_launch();
-  return cudaGetLastError();
+  return tree_refit(t, lo, hi, st);
 }
 
 }  // namespace edp
@@ -383,15 +440,4 @@ thread_local int64_t g_launches = 0;
 }
 void note_launch() { ++g_launches; }
 int64_t launch_count() { return g_launches; }
-}  // namespace edp
-
-namespace edp {
-cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st) {
-  const unsigned g = grid_for(t.leaves_cap, 256) < 4 * 148 ? grid_for(t.leaves_cap, 256) : 4 * 148;
-  k_tree_leaves<<<g, 256, 0, st>>>(t.lo, t.hi, t.ids, lo, hi, t.count, t.size, t.flags);
-  note_launch();
-  k_tree_refit<<<g, 256, 0, st>>>(t.lo, t.hi, t.size, t.flags);
-  note_launch();
-  return cudaGetLastError();
-}
 }  // namespace edp
