@@ -204,6 +204,84 @@ __device__ inline int query_next(const Tree &t, int leaves, float4 lo, float4 hi
   return node;
 }
 
+// ---------------------------------------------------------------- warp walk
+// A warp walks the tree 32 nodes at a time: the descendants of node k five
+// levels down are the contiguous nodes 32k .. 32k+31, so one step is one
+// coalesced 1 KB load and one ballot.  The first group sits r = 1..5 levels
+// below the root so that every later group, leaf groups included, is 32 wide.
+// Groups are expanded depth first, lowest lane first, so leaf batches come out
+// in increasing leaf order: the candidates, and their order, are exactly those
+// of the binary successor walk above.  Only leaves at or after `cursor` are
+// produced.  Every member is warp-uniform; all 32 lanes must call together.
+struct WarpWalk {
+  int levels;      // leaves = 2^levels
+  int top;         // level of the first group
+  int depth, level, base, width;
+  unsigned pending[8];  // overlapping, not yet expanded nodes per depth (lane bits)
+};
+
+__device__ inline unsigned walk_test(const Tree &t, int leaves, const WarpWalk &w, float4 lo,
+                                     float4 hi, int cursor) {
+  const int lane = threadIdx.x & 31;
+  bool hit = false;
+  if (lane < w.width) {
+    const int node = w.base + lane;
+    const int last = ((node + 1) << (w.levels - w.level)) - leaves - 1;  // last leaf below
+    if (last >= cursor) hit = overlaps(__ldg(&t.nodes[2 * node]), __ldg(&t.nodes[2 * node + 1]), lo, hi);
+  }
+  return __ballot_sync(0xffffffffu, hit);
+}
+
+__device__ inline void walk_begin(WarpWalk &w, const Tree &t, int leaves, float4 lo, float4 hi,
+                                  int cursor) {
+  w.levels = 31 - __clz(leaves);
+  w.top = w.levels == 0 ? 0 : (w.levels - 1) % 5 + 1;
+  w.depth = 0;
+  w.level = w.top;
+  w.base = 1 << w.top;
+  w.width = 1 << w.top;
+  w.pending[0] = cursor < leaves ? walk_test(t, leaves, w, lo, hi, cursor) : 0u;
+}
+
+// Advance to the next leaf batch: bit i of `batch` marks an overlapping leaf
+// `first + i`.  Returns false when no leaf is left (resume = leaves) or when
+// `budget` group tests are spent first (resume = the first leaf not walked;
+// every overlapping leaf before it has been produced).
+__device__ inline bool walk_next(WarpWalk &w, const Tree &t, int leaves, float4 lo, float4 hi,
+                                 int cursor, int &budget, unsigned &batch, int &first,
+                                 int &resume) {
+  for (;;) {
+    if (w.level == w.levels && w.pending[w.depth] != 0) {
+      batch = w.pending[w.depth];
+      w.pending[w.depth] = 0;
+      first = w.base - leaves;
+      return true;
+    }
+    while (w.pending[w.depth] == 0) {
+      if (w.depth == 0) {
+        resume = leaves;
+        return false;
+      }
+      --w.depth;
+      w.level -= 5;
+      w.base = w.depth == 0 ? 1 << w.top : (w.base >> 5) & ~31;
+      w.width = w.depth == 0 ? 1 << w.top : 32;
+    }
+    const int node = w.base + __ffs(int(w.pending[w.depth])) - 1;
+    if (budget <= 0) {
+      resume = max(cursor, (node << (w.levels - w.level)) - leaves);
+      return false;
+    }
+    --budget;
+    w.pending[w.depth] &= w.pending[w.depth] - 1;
+    ++w.depth;
+    w.level += 5;
+    w.base = node << 5;
+    w.width = 32;
+    w.pending[w.depth] = walk_test(t, leaves, w, lo, hi, cursor);
+  }
+}
+
 // 15 bits per axis Morton code of a box centre clamped to [0,1] (kernels.py:67-91).
 __host__ __device__ inline uint32_t part1by1(uint32_t x) {
   x &= 0x0000ffffu;

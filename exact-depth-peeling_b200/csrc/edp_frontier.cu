@@ -7,153 +7,344 @@ namespace {
 
 constexpr int kBlock = 128;
 
-// Does the part of segment a->b inside the convex patch lie strictly in front
-// of it somewhere?  za, zb are patch depth minus segment depth at the ends
-// (positive: segment nearer).  Clips the parameter range by each patch edge
-// half-plane and by the depth half-plane (frontier.py:81-103).
-__device__ inline bool front_segment(const V2 *p, int n, V2 a, V2 b, double za, double zb) {
-  double low = 0.0, high = 1.0;
-  for (int j = 0; j <= n; ++j) {
-    double da = za, db = zb;
-    if (j < n) {
-      V2 u = p[j], v = p[(j + 1) % n];
-      da = cross(u, v, a);
-      db = cross(u, v, b);
-    }
-    if (da <= 0.0 && db <= 0.0) return false;
-    if (da < 0.0) low = fmax(low, da / (da - db));
-    if (db < 0.0) high = fmin(high, da / (da - db));
-  }
-  return high > low;
+constexpr int kWarps = kBlock / 32;
+constexpr unsigned kFull = 0xffffffffu;
+// Group tests one patch may spend per round before it carries over.  The
+// budget decides only how the work is spread over rounds, never which cut a
+// patch takes: every patch meets its candidates in leaf order in any case.
+constexpr int kStepBudget = 48;
+
+__device__ inline V2 shfl(V2 x, int lane) {
+  return v2(__shfl_sync(kFull, x.x, lane), __shfl_sync(kFull, x.y, lane));
 }
 
-// One frontier round.  Each patch visits at most kCandidatesPerPass contour
-// segments of the segment hierarchy, continuing from its cursor.  The first
-// segment that crosses the patch interior and is nearer somewhere splits the
-// patch along its supporting line into two next-round patches that inherit the
-// cursor; a patch whose traversal completes is final and goes to the output
-// pool; otherwise it carries over (frontier.py:106-223).  Slots are reserved
-// once per converged group of threads and counters are flushed once per thread.
+// polygon_bounds() of the patch held one vertex per lane (min and max are
+// exact, so the butterfly order does not matter).
+__device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4 &lo, float4 &hi) {
+  const bool mine = int(threadIdx.x & 31) < n;
+  const double z = value(score, p);
+  double lx = mine ? p.x : 1.0e30, ly = mine ? p.y : 1.0e30, lz = mine ? z : 1.0e30;
+  double hx = mine ? p.x : -1.0e30, hy = mine ? p.y : -1.0e30, hz = mine ? z : -1.0e30;
+  for (int off = 16; off > 0; off >>= 1) {
+    lx = fmin(lx, __shfl_xor_sync(kFull, lx, off));
+    ly = fmin(ly, __shfl_xor_sync(kFull, ly, off));
+    lz = fmin(lz, __shfl_xor_sync(kFull, lz, off));
+    hx = fmax(hx, __shfl_xor_sync(kFull, hx, off));
+    hy = fmax(hy, __shfl_xor_sync(kFull, hy, off));
+    hz = fmax(hz, __shfl_xor_sync(kFull, hz, off));
+  }
+  double pz = 2.0e-7 * fmax(1.0, fmax(fabs(lz), fabs(hz)));
+  lo = make_float4(float(lx - 2.0e-7), float(ly - 2.0e-7), float(lz - pz), 0.f);
+  hi = make_float4(float(hx + 2.0e-7), float(hy + 2.0e-7), float(hz + pz), 0.f);
+}
+
+// Does segment a->b cut the patch?  Its line has patch vertices strictly on
+// both sides, and the part of the segment inside the patch lies strictly in
+// front of it somewhere: the segment's parameter range clipped by each patch
+// edge and by the depth half-plane stays open (frontier.py:81-103).  za, zb
+// are patch depth minus segment depth at the ends (positive: segment nearer).
+//
+// Two layouts of the same test.  For a dense batch each lane takes one
+// candidate and walks the patch, whose vertices reach it by shuffle.  For a
+// sparse batch the warp takes the candidates one by one with a lane per patch
+// edge (p -> q): ballots decide the sides and the closed edges, and warp
+// maxima / minima give the clip range.  Both are exact restatements: the
+// clip range is a max / min of the same quotients, which is order-free.
+constexpr int kDenseBatch = 8;
+
+// The contour segments: hierarchy leaf ids, end points and depth at the ends.
+struct Segments {
+  const int *ids;
+  const V2 *a, *b, *near;
+};
+
+__device__ __noinline__ unsigned cutting_lanes(Segments g, unsigned batch, int first, V2 p, int n,
+                                               const Plane &sc, V2 &a, V2 &b) {
+  const int lane = threadIdx.x & 31;
+  const bool mine = (batch >> lane) & 1u;
+  a = v2(0.0, 0.0);
+  b = a;
+  double za = 0.0, zb = 0.0;
+  if (mine) {
+    const int c = __ldg(&g.ids[first + lane]);
+    a = g.a[c];
+    b = g.b[c];
+    const V2 near = g.near[c];
+    za = value(sc, a) - near.x;
+    zb = value(sc, b) - near.y;
+  }
+  bool positive = false, negative = false, open = true;
+  double low = 0.0, high = 1.0;
+  const V2 start = shfl(p, 0);
+  V2 u = start;
+  for (int j = 0; j < n; ++j) {
+    const V2 v = j + 1 < n ? shfl(p, j + 1) : start;
+    const double side = cross(a, b, u);
+    positive |= side > 0.0;
+    negative |= side < 0.0;
+    const double da = cross(u, v, a), db = cross(u, v, b);
+    if (da <= 0.0 && db <= 0.0) open = false;
+    const double r = da / (da - db);
+    if (da < 0.0) low = fmax(low, r);
+    if (db < 0.0) high = fmin(high, r);
+    u = v;
+  }
+  if (za <= 0.0 && zb <= 0.0) open = false;
+  const double rz = za / (za - zb);
+  if (za < 0.0) low = fmax(low, rz);
+  if (zb < 0.0) high = fmin(high, rz);
+  return __ballot_sync(kFull, mine && positive && negative && open && high > low);
+}
+
+// First cutting lane of a sparse batch, or -1; a, b are its segment.
+__device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 q, int n,
+                                const Plane &sc, V2 &a, V2 &b) {
+  const bool mine = int(threadIdx.x & 31) < n;
+  while (batch) {
+    const int k = __ffs(int(batch)) - 1;
+    batch &= batch - 1;
+    const int c = __ldg(&g.ids[first + k]);
+    a = g.a[c];
+    b = g.b[c];
+    const double side = cross(a, b, p);
+    if (!__ballot_sync(kFull, mine && side > 0.0) || !__ballot_sync(kFull, mine && side < 0.0))
+      continue;
+    const V2 near = g.near[c];
+    const double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
+    if (za <= 0.0 && zb <= 0.0) continue;
+    const double da = cross(p, q, a), db = cross(p, q, b);
+    if (__ballot_sync(kFull, mine && da <= 0.0 && db <= 0.0)) continue;
+    const double r = da / (da - db);
+    double low = mine && da < 0.0 ? fmax(0.0, r) : 0.0;
+    double high = mine && db < 0.0 ? fmin(1.0, r) : 1.0;
+    for (int off = 16; off > 0; off >>= 1) {
+      low = fmax(low, __shfl_xor_sync(kFull, low, off));
+      high = fmin(high, __shfl_xor_sync(kFull, high, off));
+    }
+    const double rz = za / (za - zb);
+    if (za < 0.0) low = fmax(low, rz);
+    if (zb < 0.0) high = fmin(high, rz);
+    if (high > low) return k;
+  }
+  return -1;
+}
+
+// clean() of the polygon held one vertex per lane (x, m <= kMaxVertices
+// vertices).  When no two consecutive points are near duplicates every point
+// stays and only the closing merge and the area / perimeter test remain; their
+// sums run in the sequential order through shuffles, so they round exactly as
+// clean() does.  Otherwise lane 0 runs clean() itself on `buf` (a per-warp
+// scratch of kMaxVertices points).  Returns the new size; x holds the result.
+__device__ __noinline__ int serial_clean(V2 &x, int m, V2 *buf) {
+  const int lane = threadIdx.x & 31;
+  if (lane < m) buf[lane] = x;
+  __syncwarp();
+  int count = 0;
+  if (lane == 0) count = clean(buf, m);
+  __syncwarp();
+  count = __shfl_sync(kFull, count, 0);
+  if (lane < count) x = buf[lane];
+  __syncwarp();
+  return count;
+}
+
+__device__ inline int warp_clean(V2 &x, int m, V2 *buf) {
+  const int lane = threadIdx.x & 31;
+  const double merge = kEps * 0.01;
+  const V2 prev = shfl(x, lane > 0 ? lane - 1 : 0);
+  const bool near = lane > 0 && lane < m && !(length(x - prev) > merge);
+  if (__ballot_sync(kFull, near)) return serial_clean(x, m, buf);
+  int count = m;
+  if (count > 1 && length(shfl(x, 0) - shfl(x, count - 1)) <= merge) --count;
+  if (count < 3) return 0;
+  const V2 origin = shfl(x, 0), next = shfl(x, lane + 1 < count ? lane + 1 : 0);
+  const double term = cross(origin, x, next);
+  const double step = fabs(next.x - x.x) + fabs(next.y - x.y);
+  double area2 = 0.0, perimeter = 0.0;
+  for (int j = 0; j < count; ++j) {
+    area2 += __shfl_sync(kFull, term, j);
+    perimeter += __shfl_sync(kFull, step, j);
+  }
+  return area2 <= kEps * perimeter ? 0 : count;
+}
+
+// Split the patch (one vertex per lane, q the next vertex) by the supporting
+// line of a->b into the part on the left (pl, nl) and on the right (pr, nr),
+// both cleaned: the vertex sequence of the sequential split (kernels.py:184-203)
+// placed with ballots and prefix counts.  Returns false when a part exceeds
+// kMaxVertices.
+__device__ inline bool warp_split(V2 p, V2 q, int n, V2 a, V2 b, V2 *left, V2 *right, V2 &pl,
+                                  int &nl, V2 &pr, int &nr) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const V2 dir = b - a;
+  const Plane s{-dir.y, dir.x, 0.0, 0.0};
+  const bool mine = lane < n;
+  const double du = value(s, p - a);
+  const double dv = __shfl_sync(kFull, du, lane + 1 < n ? lane + 1 : 0);
+  const bool in = mine && du >= 0.0, out = mine && du <= 0.0;
+  const bool cut = mine && ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0));
+  const unsigned bin = __ballot_sync(kFull, in), bout = __ballot_sync(kFull, out);
+  const unsigned bcut = __ballot_sync(kFull, cut);
+  nl = __popc(bin) + __popc(bcut);
+  nr = __popc(bout) + __popc(bcut);
+  if (nl > kMaxVertices || nr > kMaxVertices) return false;
+  const int at_l = __popc(bin & below) + __popc(bcut & below);
+  const int at_r = __popc(bout & below) + __popc(bcut & below);
+  if (in) left[at_l] = p;
+  if (out) right[at_r] = p;
+  if (cut) {
+    const V2 x = p + (du / (du - dv)) * (q - p);
+    left[at_l + (in ? 1 : 0)] = x;
+    right[at_r + (out ? 1 : 0)] = x;
+  }
+  __syncwarp();
+  pl = left[lane];
+  pr = right[lane];
+  __syncwarp();
+  nl = warp_clean(pl, nl, left);
+  nr = warp_clean(pr, nr, right);
+  return true;
+}
+
+// The next round's frontier.
+struct Frontier {
+  V2 *v;
+  int *n, *src, *cur;
+  int *count, *status;
+  int64_t capacity;
+};
+
+// Append a patch (one vertex per lane) to the next frontier; false on overflow.
+__device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int cursor) {
+  const int lane = threadIdx.x & 31;
+  int slot = 0;
+  if (lane == 0) slot = atomicAdd(f.count, 1);
+  slot = __shfl_sync(kFull, slot, 0);
+  if (slot >= f.capacity) {
+    if (lane == 0) set_error(f.status, kErrResidual);
+    return false;
+  }
+  if (lane < n) f.v[int64_t(kMaxVertices) * slot + lane] = p;
+  if (lane == 0) {
+    f.n[slot] = n;
+    f.src[slot] = source;
+    f.cur[slot] = cursor;
+  }
+  return true;
+}
+
+// One frontier round, one patch per warp (frontier.py:106-223).  A patch
+// meets the contour segments whose boxes overlap its own in leaf order,
+// starting at its cursor (the first leaf it has not met).  The first segment
+// that cuts it splits it along the segment's line: the right part goes to the
+// next round, the left part continues in this warp, both with the cursor just
+// past the cutting leaf (a collapsed part cancels the cut and the patch
+// continues).  The continuing part keeps its walk: only the cut's leaf group
+// is tested again, against the part's box; pending groups above it are
+// tested against the part's box when they are expanded.  A patch that has
+// met every candidate is final and goes to the output pool; one that spends
+// its budget carries over.  Warps take patches from a shared counter.
 __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
-  enum Action { kSkip = 0, kSplit = 1, kCarry = 2, kDone = 3 };
+  __shared__ V2 s_parts[kWarps][2][kMaxVertices];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  V2 *left_part = s_parts[warp][0], *right_part = s_parts[warp][1];
   const int par = *d.parity;
   const V2 *fv = d.fv[par];
   const int *fn = d.fn[par], *fsrc = d.fsrc[par], *fcur = d.fcur[par];
-  V2 *nv = d.fv[par ^ 1];
-  int *nn = d.fn[par ^ 1], *nsrc = d.fsrc[par ^ 1], *ncur = d.fcur[par ^ 1];
   const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
   const int leaves = *d.seg_tree.size;
-  long long visits = 0, tests = 0, splits = 0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < live;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    if (d.status[kError] != 0) return;
-    const int n = fn[i];
+  const int next_lane = lane + 1;
+  const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near};
+  const Frontier next{d.fv[par ^ 1], d.fn[par ^ 1], d.fsrc[par ^ 1], d.fcur[par ^ 1],
+                      &d.status[kNextResidual], d.status, d.cap.frontier};
+  long long visits = 0, tests = 0, splits = 0;  // lane 0's tallies
+  for (;;) {
+    int i = 0, failed = 0;
+    if (lane == 0) {
+      i = atomicAdd(&d.sc[kFrontierNext], 1);
+      failed = *(volatile int *)&d.status[kError];
+    }
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= live || __shfl_sync(kFull, failed, 0) != 0) break;
+    int n = fn[i];
     if (n == 0) continue;
     ++visits;
     const int source = fsrc[i];
-    int node = fcur[i];
-    const V2 *p = fv + int64_t(kMaxVertices) * i;
+    int cursor = fcur[i];
+    V2 p = lane < n ? fv[int64_t(kMaxVertices) * i + lane] : v2(0.0, 0.0);
+    V2 q = shfl(p, next_lane < n ? next_lane : 0);
     const Plane sc = d.scores[source];
+    int budget = kStepBudget;
     float4 lo, hi;
-    polygon_bounds(p, n, sc, lo, hi);
+    warp_bounds(p, n, sc, lo, hi);
     lo.z = -1.0e30f;
-    int action = kCarry;
-    V2 a = v2(0.0, 0.0), b = a;
-    for (int task = 0; task < kCandidatesPerPass; ++task) {
-      int c;
-      node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
-      if (c < 0) {
-        action = kDone;
+    WarpWalk w;
+    walk_begin(w, d.seg_tree, leaves, lo, hi, cursor);
+    for (;;) {
+      unsigned batch;
+      int first, resume = leaves, cut = -1;
+      V2 a, b;
+      while (walk_next(w, d.seg_tree, leaves, lo, hi, cursor, budget, batch, first, resume)) {
+        const int count = __popc(batch);
+        if (count >= kDenseBatch) {
+          const unsigned cuts = cutting_lanes(segs, batch, first, p, n, sc, a, b);
+          if (cuts) {
+            cut = __ffs(int(cuts)) - 1;
+            a = shfl(a, cut);
+            b = shfl(b, cut);
+          }
+        } else {
+          cut = first_cut(segs, batch, first, p, q, n, sc, a, b);
+        }
+        tests += cut >= 0 ? __popc(batch & (kFull >> (31 - cut))) : count;  // met up to the cut
+        if (cut >= 0) break;
+      }
+      if (cut < 0) {
+        if (resume < leaves) {
+          push_patch(next, p, n, source, resume);
+          break;
+        }
+        int out = 0;
+        if (lane == 0) out = atomicAdd(&d.status[kPolygons], 1);
+        out = __shfl_sync(kFull, out, 0);
+        if (out >= d.cap.regions) {
+          if (lane == 0) set_error(d.status, kErrOutput);
+          break;
+        }
+        if (lane < n) d.out_v[int64_t(kMaxVertices) * out + lane] = p;
+        if (lane == 0) {
+          d.out_n[out] = n;
+          d.out_src[out] = source;
+          d.out_layer[out] = 0;
+        }
         break;
       }
-      ++tests;
-      a = d.seg_a[c];
-      b = d.seg_b[c];
-      bool positive = false, negative = false;
-      for (int j = 0; j < n; ++j) {
-        double side = cross(a, b, p[j]);
-        positive |= side > 0.0;
-        negative |= side < 0.0;
-      }
-      if (!(positive && negative)) continue;
-      const V2 near = d.seg_near[c];
-      double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
-      if (front_segment(p, n, a, b, za, zb)) {
-        action = kSplit;
+      cursor = first + cut + 1;
+      V2 pl, pr;
+      int nl, nr;
+      if (!warp_split(p, q, n, a, b, left_part, right_part, pl, nl, pr, nr)) {
+        if (lane == 0) set_error(d.status, kErrPolygon);
         break;
       }
-    }
-    const int slot = reserve(&d.status[kNextResidual],
-                             action == kSplit ? 2 : action == kCarry ? 1 : 0);
-    const int out = reserve(&d.status[kPolygons], action == kDone ? 1 : 0);
-    if (action == kDone) {
-      if (out >= d.cap.regions) {
-        set_error(d.status, kErrOutput);
-        continue;
+      if (nl > 0 && nr > 0) {
+        ++splits;
+        if (!push_patch(next, pr, nr, source, cursor)) break;
+        p = pl;
+        n = nl;
+        q = shfl(p, next_lane < n ? next_lane : 0);
+        warp_bounds(p, n, sc, lo, hi);
+        lo.z = -1.0e30f;
       }
-      V2 *dst = d.out_v + int64_t(kMaxVertices) * out;
-      for (int j = 0; j < n; ++j) dst[j] = p[j];
-      d.out_n[out] = n;
-      d.out_src[out] = source;
-      d.out_layer[out] = 0;
-      continue;
+      w.pending[w.depth] = walk_test(d.seg_tree, leaves, w, lo, hi, cursor);
+      __syncwarp();  // the part buffers are rewritten by the next cut
     }
-    if (action == kCarry) {
-      if (slot >= d.cap.frontier) {
-        set_error(d.status, kErrResidual);
-        continue;
-      }
-      V2 *dst = nv + int64_t(kMaxVertices) * slot;
-      for (int j = 0; j < n; ++j) dst[j] = p[j];
-      nn[slot] = n;
-      nsrc[slot] = source;
-      ncur[slot] = node;
-      continue;
-    }
-    if (int64_t(slot) + 1 >= d.cap.frontier) {
-      set_error(d.status, kErrResidual);
-      continue;
-    }
-    V2 *left_v = nv + int64_t(kMaxVertices) * slot;
-    V2 *right_v = left_v + kMaxVertices;
-    int left = 0, right = 0;
-    V2 dir = b - a;
-    Plane s{-dir.y, dir.x, 0.0, 0.0};
-    for (int j = 0; j < n; ++j) {
-      V2 u = p[j], v = p[(j + 1) % n];
-      double du = value(s, u - a), dv = value(s, v - a);
-      if (du >= 0.0) left = append(left_v, left, u);
-      if (du <= 0.0) right = append(right_v, right, u);
-      if ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0)) {
-        V2 x = u + (du / (du - dv)) * (v - u);
-        left = append(left_v, left, x);
-        right = append(right_v, right, x);
-      }
-    }
-    left = clean(left_v, left);
-    right = clean(right_v, right);
-    if (left > kMaxVertices || right > kMaxVertices) {
-      set_error(d.status, kErrPolygon);
-      continue;
-    }
-    if (left > 0 && right > 0) {
-      ++splits;
-    } else {
-      // A collapsed child cancels this cut; the parent continues next round.
-      left = n;
-      right = 0;
-      for (int j = 0; j < n; ++j) left_v[j] = p[j];
-    }
-    nn[slot] = left;
-    nn[slot + 1] = right;
-    nsrc[slot] = source;
-    nsrc[slot + 1] = source;
-    ncur[slot] = node;
-    ncur[slot + 1] = node;
   }
-  count_add(&d.metrics[kTargetVisits], visits);
-  count_add(&d.metrics[kContourTests], tests);
-  count_add(&d.metrics[kSplits], splits);
+  if (lane == 0) {
+    count_add(&d.metrics[kTargetVisits], visits);
+    count_add(&d.metrics[kContourTests], tests);
+    count_add(&d.metrics[kSplits], splits);
+  }
 }
 
 // Swap frontiers and decide whether another round runs (event_kernels.py:12-25).
@@ -161,6 +352,7 @@ __global__ void k_advance(Dev d) {
   int next = d.status[kNextResidual];
   d.status[kResidual] = next;
   d.status[kNextResidual] = 0;
+  d.sc[kFrontierNext] = 0;
   long long rounds = ++d.metrics[kRounds];
   if (rounds >= d.cap.rounds && next > 0) set_error(d.status, kErrRounds);
   d.status[kPeakResidual] = max(d.status[kPeakResidual], next);
@@ -173,8 +365,8 @@ __global__ void k_advance(Dev d) {
 }  // namespace
 
 cudaError_t stage_step(const Dev &d, cudaStream_t st) {
-  int64_t g = ceil_div(d.cap.frontier, kBlock);
-  if (g > 148 * 32) g = 148 * 32;
+  int64_t g = ceil_div(d.cap.frontier, kWarps);
+  if (g > 148 * 8) g = 148 * 8;
   k_subdivide<<<unsigned(g), kBlock, 0, st>>>(d);
   note_launch();
   k_advance<<<1, 1, 0, st>>>(d);

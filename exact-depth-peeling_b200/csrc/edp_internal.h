@@ -94,6 +94,7 @@ enum Scalar : int {
   kSegmentCount = 5,   // 8 n (constant)
   kFrontierLive = 6,   // min(status[0], frontier)
   kUniqueVertices = 7, // distinct (layer, point) boundary vertices
+  kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 16
 };
 

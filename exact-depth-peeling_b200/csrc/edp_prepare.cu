@@ -354,12 +354,13 @@ __global__ void k_seed(Dev d) {
     for (int j = 0; j < n; ++j) dst[j] = src[j];
     d.fn[0][i] = n;
     d.fsrc[0][i] = int(i);
-    d.fcur[0][i] = 1;
+    d.fcur[0][i] = 0;  // first contour leaf not yet met
   }
   if (tid() == 0) {
     if (!fits) set_error(d.status, kErrResidual);
     d.status[kResidual] = fits ? d.n : 0;
     d.status[kPeakResidual] = d.status[kResidual];
+    d.sc[kFrontierNext] = 0;
   }
 }
 
