@@ -44,13 +44,11 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
 // edge and by the depth half-plane stays open (frontier.py:81-103).  za, zb
 // are patch depth minus segment depth at the ends (positive: segment nearer).
 //
-// Two layouts of the same test.  For a dense batch each lane takes one
-// candidate and walks the patch, whose vertices reach it by shuffle.  For a
-// sparse batch the warp takes the candidates one by one with a lane per patch
-// edge (p -> q): ballots decide the sides and the closed edges, and warp
-// maxima / minima give the clip range.  Both are exact restatements: the
-// clip range is a max / min of the same quotients, which is order-free.
-constexpr int kDenseBatch = 8;
+// The warp takes a batch's candidates one by one in leaf order with a lane per
+// patch edge (p -> q): ballots decide the sides and the closed edges, and warp
+// maxima / minima give the clip range, which is a max / min of the same
+// quotients as the sequential clip and so is order-free.  Each lane first
+// loads one candidate of the batch, so the loop itself reads no memory.
 
 // The contour segments: hierarchy leaf ids, end points and depth at the ends.
 struct Segments {
@@ -58,58 +56,27 @@ struct Segments {
   const V2 *a, *b, *near;
 };
 
-__device__ __noinline__ unsigned cutting_lanes(Segments g, unsigned batch, int first, V2 p, int n,
-                                               const Plane &sc, V2 &a, V2 &b) {
-  const int lane = threadIdx.x & 31;
-  const bool mine = (batch >> lane) & 1u;
-  a = v2(0.0, 0.0);
-  b = a;
-  double za = 0.0, zb = 0.0;
-  if (mine) {
-    const int c = __ldg(&g.ids[first + lane]);
-    a = g.a[c];
-    b = g.b[c];
-    const V2 near = g.near[c];
-    za = value(sc, a) - near.x;
-    zb = value(sc, b) - near.y;
-  }
-  bool positive = false, negative = false, open = true;
-  double low = 0.0, high = 1.0;
-  const V2 start = shfl(p, 0);
-  V2 u = start;
-  for (int j = 0; j < n; ++j) {
-    const V2 v = j + 1 < n ? shfl(p, j + 1) : start;
-    const double side = cross(a, b, u);
-    positive |= side > 0.0;
-    negative |= side < 0.0;
-    const double da = cross(u, v, a), db = cross(u, v, b);
-    if (da <= 0.0 && db <= 0.0) open = false;
-    const double r = da / (da - db);
-    if (da < 0.0) low = fmax(low, r);
-    if (db < 0.0) high = fmin(high, r);
-    u = v;
-  }
-  if (za <= 0.0 && zb <= 0.0) open = false;
-  const double rz = za / (za - zb);
-  if (za < 0.0) low = fmax(low, rz);
-  if (zb < 0.0) high = fmin(high, rz);
-  return __ballot_sync(kFull, mine && positive && negative && open && high > low);
-}
-
-// First cutting lane of a sparse batch, or -1; a, b are its segment.
+// First cutting lane of a batch, or -1; a, b are its segment.
 __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 q, int n,
                                 const Plane &sc, V2 &a, V2 &b) {
-  const bool mine = int(threadIdx.x & 31) < n;
+  const int lane = threadIdx.x & 31;
+  const bool mine = lane < n;
+  V2 ca = v2(0.0, 0.0), cb = ca, cn = ca;
+  if ((batch >> lane) & 1u) {
+    const int c = __ldg(&g.ids[first + lane]);
+    ca = g.a[c];
+    cb = g.b[c];
+    cn = g.near[c];
+  }
   while (batch) {
     const int k = __ffs(int(batch)) - 1;
     batch &= batch - 1;
-    const int c = __ldg(&g.ids[first + k]);
-    a = g.a[c];
-    b = g.b[c];
+    a = shfl(ca, k);
+    b = shfl(cb, k);
     const double side = cross(a, b, p);
     if (!__ballot_sync(kFull, mine && side > 0.0) || !__ballot_sync(kFull, mine && side < 0.0))
       continue;
-    const V2 near = g.near[c];
+    const V2 near = shfl(cn, k);
     const double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
     if (za <= 0.0 && zb <= 0.0) continue;
     const double da = cross(p, q, a), db = cross(p, q, b);
@@ -286,18 +253,8 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
       int first, resume = leaves, cut = -1;
       V2 a, b;
       while (walk_next(w, d.seg_tree, leaves, lo, hi, cursor, budget, batch, first, resume)) {
-        const int count = __popc(batch);
-        if (count >= kDenseBatch) {
-          const unsigned cuts = cutting_lanes(segs, batch, first, p, n, sc, a, b);
-          if (cuts) {
-            cut = __ffs(int(cuts)) - 1;
-            a = shfl(a, cut);
-            b = shfl(b, cut);
-          }
-        } else {
-          cut = first_cut(segs, batch, first, p, q, n, sc, a, b);
-        }
-        tests += cut >= 0 ? __popc(batch & (kFull >> (31 - cut))) : count;  // met up to the cut
+        cut = first_cut(segs, batch, first, p, q, n, sc, a, b);
+        tests += __popc(cut >= 0 ? batch & (kFull >> (31 - cut)) : batch);  // met up to the cut
         if (cut >= 0) break;
       }
       if (cut < 0) {
