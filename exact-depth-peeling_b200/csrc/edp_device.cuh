@@ -217,7 +217,31 @@ struct WarpWalk {
   int levels;      // leaves = 2^levels
   int top;         // level of the first group
   int depth, level, base, width;
-  unsigned pending[8];  // overlapping, not yet expanded nodes per depth (lane bits)
+  // Overlapping, not yet expanded nodes per depth (lane bits).  Leaves fit an
+  // int, so there are at most 30 levels and depths 0..5; the depth is
+  // warp-uniform, so named registers and a uniform switch keep the stack out
+  // of local memory.
+  unsigned p0, p1, p2, p3, p4, p5;
+  __device__ unsigned pending() const {
+    switch (depth) {
+      case 0: return p0;
+      case 1: return p1;
+      case 2: return p2;
+      case 3: return p3;
+      case 4: return p4;
+      default: return p5;
+    }
+  }
+  __device__ void set_pending(unsigned v) {
+    switch (depth) {
+      case 0: p0 = v; break;
+      case 1: p1 = v; break;
+      case 2: p2 = v; break;
+      case 3: p3 = v; break;
+      case 4: p4 = v; break;
+      default: p5 = v; break;
+    }
+  }
 };
 
 __device__ inline unsigned walk_test(const Tree &t, int leaves, const WarpWalk &w, float4 lo,
@@ -240,7 +264,8 @@ __device__ inline void walk_begin(WarpWalk &w, const Tree &t, int leaves, float4
   w.level = w.top;
   w.base = 1 << w.top;
   w.width = 1 << w.top;
-  w.pending[0] = cursor < leaves ? walk_test(t, leaves, w, lo, hi, cursor) : 0u;
+  w.p1 = w.p2 = w.p3 = w.p4 = w.p5 = 0u;
+  w.p0 = cursor < leaves ? walk_test(t, leaves, w, lo, hi, cursor) : 0u;
 }
 
 // Advance to the next leaf batch: bit i of `batch` marks an overlapping leaf
@@ -251,13 +276,14 @@ __device__ inline bool walk_next(WarpWalk &w, const Tree &t, int leaves, float4 
                                  int cursor, int &budget, unsigned &batch, int &first,
                                  int &resume) {
   for (;;) {
-    if (w.level == w.levels && w.pending[w.depth] != 0) {
-      batch = w.pending[w.depth];
-      w.pending[w.depth] = 0;
+    unsigned pending = w.pending();
+    if (w.level == w.levels && pending != 0) {
+      batch = pending;
+      w.set_pending(0u);
       first = w.base - leaves;
       return true;
     }
-    while (w.pending[w.depth] == 0) {
+    while (pending == 0) {
       if (w.depth == 0) {
         resume = leaves;
         return false;
@@ -266,19 +292,20 @@ __device__ inline bool walk_next(WarpWalk &w, const Tree &t, int leaves, float4 
       w.level -= 5;
       w.base = w.depth == 0 ? 1 << w.top : (w.base >> 5) & ~31;
       w.width = w.depth == 0 ? 1 << w.top : 32;
+      pending = w.pending();
     }
-    const int node = w.base + __ffs(int(w.pending[w.depth])) - 1;
+    const int node = w.base + __ffs(int(pending)) - 1;
     if (budget <= 0) {
       resume = max(cursor, (node << (w.levels - w.level)) - leaves);
       return false;
     }
     --budget;
-    w.pending[w.depth] &= w.pending[w.depth] - 1;
+    w.set_pending(pending & (pending - 1));
     ++w.depth;
     w.level += 5;
     w.base = node << 5;
     w.width = 32;
-    w.pending[w.depth] = walk_test(t, leaves, w, lo, hi, cursor);
+    w.set_pending(walk_test(t, leaves, w, lo, hi, cursor));
   }
 }
 

@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
         warp_bounds(p, n, sc, lo, hi);
         lo.z = -1.0e30f;
       }
-      w.pending[w.depth] = walk_test(d.seg_tree, leaves, w, lo, hi, cursor);
+      w.set_pending(walk_test(d.seg_tree, leaves, w, lo, hi, cursor));
       __syncwarp();  // the part buffers are rewritten by the next cut
     }
   }

@@ -169,6 +169,11 @@ struct Dev {
   int *point_table;
   int point_mask;
   float4 *pt_lo, *pt_hi;
+  // Output polygons in (layer, Morton code of the box centre) order: the
+  // noding kernel walks them in this order so that neighbouring threads walk
+  // neighbouring parts of the point hierarchy.
+  uint64_t *mesh_keys, *mesh_keys_tmp;
+  int *mesh_order, *mesh_order_tmp;
   V2 *tri_uv;        // [triangles][3]
   double *tri_world; // [triangles][3][3]
   int *tri_src, *tri_layer;

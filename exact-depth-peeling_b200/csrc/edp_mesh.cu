@@ -73,6 +73,28 @@ __global__ void k_scatter(Dev d) {
   }
 }
 
+// Sort key of each live output polygon: its layer above the 15-bit Morton
+// code of its box centre, the key layout of the point hierarchy
+// (kernels.py:67-91).  The order only groups work; no result depends on it.
+__global__ void k_mesh_keys(Dev d) {
+  const int live = d.sc[kLivePolygons];
+  for (int64_t i = tid(); i < live; i += stride()) {
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    const int n = min(max(d.out_n[i], 1), kMaxVertices);
+    double lx = p[0].x, ly = p[0].y, hx = p[0].x, hy = p[0].y;
+    for (int j = 1; j < n; ++j) {
+      lx = fmin(lx, p[j].x); ly = fmin(ly, p[j].y);
+      hx = fmax(hx, p[j].x); hy = fmax(hy, p[j].y);
+    }
+    const float cx = fminf(fmaxf(float(0.5 * (lx + hx)), 0.f), 1.f);
+    const float cy = fminf(fmaxf(float(0.5 * (ly + hy)), 0.f), 1.f);
+    const uint32_t x = uint32_t(int(cx * 32767.0f)), y = uint32_t(int(cy * 32767.0f));
+    d.mesh_keys[i] = (uint64_t(uint32_t(d.out_layer[i]) & 0xffffu) << 32) |
+                     uint64_t(part1by1(x) | (part1by1(y) << 1));
+    d.mesh_order[i] = int(i);
+  }
+}
+
 // World position of a window point on a source plane (kernels.py:994-1006).
 __device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
   const double *st = d.settings, *m = d.inverse;
@@ -100,8 +122,9 @@ __global__ void __launch_bounds__(kBlock) k_mesh_polygons(Dev d, int edge_capaci
   const int leaves = *d.point_tree.size;
   double split_t[kPolygonSplits];
   unsigned char split_edge[kPolygonSplits];
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
+    const int64_t i = d.mesh_order[k];
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
     const int n = d.out_n[i];
     if (n < 3) continue;
@@ -249,6 +272,11 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
+  k_mesh_keys<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
+  // Layers fit 16 bits (at most 65536), so 48 key bits order the polygons.
+  EDP_CHECK(sort_pairs_u64(d.mesh_keys, d.mesh_keys_tmp, d.mesh_order, d.mesh_order_tmp,
+                           d.sc + kLivePolygons, R, 48, s, st));
   return cudaGetLastError();
 }
 
