@@ -169,11 +169,12 @@ struct Dev {
   int *point_table;
   int point_mask;
   float4 *pt_lo, *pt_hi;
-  // Output polygons in (layer, Morton code of the box centre) order: the
-  // noding kernel walks them in this order so that neighbouring threads walk
-  // neighbouring parts of the point hierarchy.
-  uint64_t *mesh_keys, *mesh_keys_tmp;
-  int *mesh_order, *mesh_order_tmp;
+  // A processing order of the live output polygons by the Morton code of
+  // their box centre (optionally below the layer), rebuilt by each stage that
+  // uses it, so that neighbouring threads walk neighbouring parts of a
+  // hierarchy.  No result depends on it.
+  uint64_t *order_keys, *order_keys_tmp;
+  int *order, *order_tmp;
   V2 *tri_uv;        // [triangles][3]
   double *tri_world; // [triangles][3][3]
   int *tri_src, *tri_layer;
@@ -216,6 +217,10 @@ cudaError_t stage_device_layer(const Dev &d, SortScratch &s, TreeBuffers &source
 // Bring the source hierarchy's leaves up to date with its item boxes without
 // re-sorting (solver.py:72-89).
 cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st);
+
+// Rebuild Dev::order over the live output polygons: by Morton code of the box
+// centre, below the layer when `layered`.
+cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStream_t st);
 
 // Stage launchers (edp_kernels.cu).  Each enqueues kernels on `st`.
 cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,

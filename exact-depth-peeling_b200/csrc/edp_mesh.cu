@@ -73,10 +73,10 @@ __global__ void k_scatter(Dev d) {
   }
 }
 
-// Sort key of each live output polygon: its layer above the 15-bit Morton
-// code of its box centre, the key layout of the point hierarchy
-// (kernels.py:67-91).  The order only groups work; no result depends on it.
-__global__ void k_mesh_keys(Dev d) {
+// Sort key of each live output polygon: the 15-bit-per-axis Morton code of
+// its box centre (the key layout of the hierarchies, kernels.py:67-91), below
+// its layer when `layered`.
+__global__ void k_order_keys(Dev d, int layered) {
   const int live = d.sc[kLivePolygons];
   for (int64_t i = tid(); i < live; i += stride()) {
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
@@ -89,9 +89,10 @@ __global__ void k_mesh_keys(Dev d) {
     const float cx = fminf(fmaxf(float(0.5 * (lx + hx)), 0.f), 1.f);
     const float cy = fminf(fmaxf(float(0.5 * (ly + hy)), 0.f), 1.f);
     const uint32_t x = uint32_t(int(cx * 32767.0f)), y = uint32_t(int(cy * 32767.0f));
-    d.mesh_keys[i] = (uint64_t(uint32_t(d.out_layer[i]) & 0xffffu) << 32) |
-                     uint64_t(part1by1(x) | (part1by1(y) << 1));
-    d.mesh_order[i] = int(i);
+    uint64_t key = part1by1(x) | (part1by1(y) << 1);
+    if (layered) key |= uint64_t(uint32_t(d.out_layer[i]) & 0xffffu) << 32;
+    d.order_keys[i] = key;
+    d.order[i] = int(i);
   }
 }
 
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kBlock) k_mesh_polygons(Dev d, int edge_capaci
   unsigned char split_edge[kPolygonSplits];
   for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
-    const int64_t i = d.mesh_order[k];
+    const int64_t i = d.order[k];
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
     const int n = d.out_n[i];
     if (n < 3) continue;
@@ -260,6 +261,15 @@ unsigned blocks(int64_t n) {
 
 }  // namespace
 
+cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStream_t st) {
+  const int64_t R = d.cap.regions;
+  k_order_keys<<<blocks(R), kBlock, 0, st>>>(d, layered ? 1 : 0);
+  note_launch();
+  // Layers fit 16 bits (at most 65536) above the 30 Morton bits.
+  return sort_pairs_u64(d.order_keys, d.order_keys_tmp, d.order, d.order_tmp,
+                        d.sc + kLivePolygons, R, layered ? 48 : 30, s, st);
+}
+
 cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
                              cudaStream_t st) {
   const int64_t R = d.cap.regions;
@@ -272,11 +282,7 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
-  k_mesh_keys<<<blocks(R), kBlock, 0, st>>>(d);
-  note_launch();
-  // Layers fit 16 bits (at most 65536), so 48 key bits order the polygons.
-  EDP_CHECK(sort_pairs_u64(d.mesh_keys, d.mesh_keys_tmp, d.mesh_order, d.mesh_order_tmp,
-                           d.sc + kLivePolygons, R, 48, s, st));
+  EDP_CHECK(order_polygons(d, true, s, st));
   return cudaGetLastError();
 }
 

@@ -417,9 +417,10 @@ __global__ void k_ray_hits(Dev d) {
   const int leaves = *d.source_tree.size;
   long long groups = 0, tests = 0;
   HitBuffer hits;
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
-    if (d.groups[i] != int(i)) continue;
+    const int i = d.order[k];  // spatial order: neighbouring rays walk neighbouring nodes
+    if (d.groups[i] != i) continue;
     V2 x = d.samples[i];
     float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
@@ -437,13 +438,13 @@ __global__ void k_ray_hits(Dev d) {
       if (node == 0) break;
     }
     d.group_counts[i] = hits.count;
-    hits.flush(d, int(i));
+    hits.flush(d, i);
     ++groups;
     const bool heavy = node > 0;
     if (heavy)
       while (node < leaves) node *= 2;
     int slot = int(reserve(&d.metrics[kHeavyRayGroups], heavy ? 1 : 0));
-    if (heavy) d.heavy_queries[slot] = make_int2(int(i), node);
+    if (heavy) d.heavy_queries[slot] = make_int2(i, node);
   }
   count_add(&d.metrics[kRayGroups], groups);
   count_add(&d.metrics[kRayCandidateTests], tests);
@@ -599,6 +600,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
     note_launch();
   }
+  EDP_CHECK(order_polygons(d, false, s, st));
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   k_heavy_hits<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);

@@ -110,10 +110,10 @@ cudaError_t allocate_shared(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.out_n, R));
   EDP_CHECK(alloc(p, &d.out_src, R));
   EDP_CHECK(alloc(p, &d.out_layer, R));
-  EDP_CHECK(alloc(p, &d.mesh_keys, R));
-  EDP_CHECK(alloc(p, &d.mesh_keys_tmp, R));
-  EDP_CHECK(alloc(p, &d.mesh_order, R));
-  EDP_CHECK(alloc(p, &d.mesh_order_tmp, R));
+  EDP_CHECK(alloc(p, &d.order_keys, R));
+  EDP_CHECK(alloc(p, &d.order_keys_tmp, R));
+  EDP_CHECK(alloc(p, &d.order, R));
+  EDP_CHECK(alloc(p, &d.order_tmp, R));
   EDP_CHECK(alloc(p, &d.counts, R));
   EDP_CHECK(alloc(p, &d.offsets, R));
   EDP_CHECK(alloc(p, &d.bverts, E));
