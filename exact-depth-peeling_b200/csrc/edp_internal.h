@@ -94,6 +94,7 @@ enum Scalar : int {
   kSegmentCount = 5,   // 8 n (constant)
   kFrontierLive = 6,   // min(status[0], frontier)
   kUniqueVertices = 7, // distinct (layer, point) boundary vertices
+  kSortHits = 8,       // hits for the global hit sort: all when a group is large, else 0
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 16
 };
@@ -162,6 +163,7 @@ struct Dev {
   int *hit_src, *hit_group, *hit_ids, *hit_ids_tmp;
   unsigned long long *hkeys, *hkeys_tmp;
   int *group_counts, *group_offsets;
+  int *group_fill;  // hits placed in each group so far
   // boundary noding and triangles
   V2 *bverts;      // per polygon vertex slot
   int *blayers;

@@ -491,12 +491,70 @@ __global__ void k_check_hits(Dev d) {
   long long total = d.metrics[kRayHits];
   if (total > d.cap.hits) set_error(d.status, kErrHits);
   d.sc[kLiveHits] = int(min(total, (long long)d.cap.hits));
+  d.sc[kSortHits] = 0;
+}
+
+// Hits of one ray group are ordered by (depth, source) within the group.  A
+// group holds one hit per source along its ray, so groups are as deep as the
+// scene's depth complexity: up to kGroupSort hits are sorted by one thread in
+// place; if any group is larger, every hit goes through the global stable
+// radix passes instead (the order is the same either way).
+constexpr int kGroupSort = 64;
+
+__global__ void k_group_sizes(Dev d) {
+  const int live = live_polygons(d);
+  bool large = false;
+  for (int64_t i = tid(); i < live; i += stride()) large |= d.group_counts[i] > kGroupSort;
+  if (__any_sync(0xffffffffu, large) && (threadIdx.x & 31) == 0) d.sc[kSortHits] = d.sc[kLiveHits];
+}
+
+// Place each hit in its group's range (group_offsets is the scan of
+// group_counts); the order inside a group is fixed by k_group_sort.
+__global__ void k_hit_place(Dev d) {
+  if (d.sc[kSortHits] != 0 || d.status[kError] != 0) return;
+  const int live = d.sc[kLiveHits];
+  for (int64_t h = tid(); h < live; h += stride()) {
+    const int g = d.hit_group[h];
+    d.hit_ids[d.group_offsets[g] + atomicAdd(&d.group_fill[g], 1)] = int(h);
+  }
+}
+
+// Order each group's hits by (ordered depth bits, source): the order of the
+// three stable radix passes below, whose keys are the same (a source is hit
+// at most once per group, so no two hits of a group tie).
+__global__ void k_group_sort(Dev d) {
+  // After a hit-pool overflow the groups' counts exceed the hits stored.
+  if (d.sc[kSortHits] != 0 || d.status[kError] != 0) return;
+  const int live = live_polygons(d);
+  for (int64_t g = tid(); g < live; g += stride()) {
+    const int k = d.group_counts[g];
+    if (k < 2) continue;
+    int *ids = d.hit_ids + d.group_offsets[g];
+    unsigned long long key[kGroupSort];
+    int src[kGroupSort], id[kGroupSort];
+    for (int j = 0; j < k; ++j) {
+      const int h = ids[j];
+      const unsigned long long kj = ordered_bits(d.hit_depth[h]);
+      const int sj = d.hit_src[h];
+      int m = j - 1;
+      while (m >= 0 && (key[m] > kj || (key[m] == kj && src[m] > sj))) {
+        key[m + 1] = key[m];
+        src[m + 1] = src[m];
+        id[m + 1] = id[m];
+        --m;
+      }
+      key[m + 1] = kj;
+      src[m + 1] = sj;
+      id[m + 1] = h;
+    }
+    for (int j = 0; j < k; ++j) ids[j] = id[j];
+  }
 }
 
 // Keys of the three stable passes that order hits by (group, depth, source)
 // (event_kernels.py:313-339, events.py:701-718).
 __global__ void k_hit_keys(Dev d, int stage) {
-  const int live = d.sc[kLiveHits];
+  const int live = d.sc[kSortHits];
   for (int64_t i = tid(); i < live; i += stride()) {
     int h = stage == 0 ? int(i) : d.hit_ids[i];
     if (stage == 0) d.hit_ids[i] = int(i);
@@ -608,14 +666,22 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
   k_check_hits<<<1, 1, 0, st>>>(d);
   note_launch();
+  k_group_sizes<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
+  // Global passes: over all hits when some group is large, else over none.
   const int pass_bits[3] = {bits_for(d.n), 64, bits_for(R)};
   for (int stage = 0; stage < 3; ++stage) {
     k_hit_keys<<<blocks(d.cap.hits), kBlock, 0, st>>>(d, stage);
     note_launch();
     EDP_CHECK(sort_pairs_u64(reinterpret_cast<uint64_t *>(d.hkeys),
                              reinterpret_cast<uint64_t *>(d.hkeys_tmp), d.hit_ids, d.hit_ids_tmp,
-                             d.sc + kLiveHits, d.cap.hits, pass_bits[stage], s, st));
+                             d.sc + kSortHits, d.cap.hits, pass_bits[stage], s, st));
   }
+  EDP_CHECK(cudaMemsetAsync(d.group_fill, 0, sizeof(int) * R, st));
+  k_hit_place<<<blocks(d.cap.hits), kBlock, 0, st>>>(d);
+  note_launch();
+  k_group_sort<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
   k_layers_reset<<<1, 1, 0, st>>>(d);
   note_launch();
   k_assign<<<blocks(R), kBlock, 0, st>>>(d);

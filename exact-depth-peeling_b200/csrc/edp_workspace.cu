@@ -180,6 +180,7 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.heavy_queries, R));
   EDP_CHECK(alloc(p, &d.group_counts, R));
   EDP_CHECK(alloc(p, &d.group_offsets, R));
+  EDP_CHECK(alloc(p, &d.group_fill, R));
   EDP_CHECK(alloc(p, &d.tasks, E));
   EDP_CHECK(alloc(p, &d.owners, E));
   EDP_CHECK(alloc(p, &d.starts, E));
