@@ -28,10 +28,8 @@ __global__ void k_mesh_check(Dev d) {
   }
 }
 
-// Boundary vertices with their layer and one noding task per polygon edge
-// (kernels.py:953-991, event_kernels.py:504-516).  Each distinct (layer,
-// point) enters the point hierarchy once: a vertex shared by several patches
-// would otherwise be a candidate of every query several times over.
+// Boundary vertices with their layer, one slot per polygon vertex
+// (kernels.py:953-991, event_kernels.py:504-516).
 __global__ void k_scatter(Dev d) {
   const int live = d.sc[kLivePolygons];
   for (int64_t i = tid(); i < live; i += stride()) {
@@ -44,31 +42,39 @@ __global__ void k_scatter(Dev d) {
       d.bverts[base + j] = p[j];
       d.blayers[base + j] = layer;
     }
-    __threadfence();  // publish the points before their slots can be found in the table
-    for (int j = 0; j < n; ++j) {
-      const int64_t slot = base + j;
-      const V2 x = p[j];
-      uint64_t h = mix64(mix64(key_bits(x.x)) ^ key_bits(x.y)) ^ mix64(uint64_t(layer) + 7ull);
-      uint32_t probe = uint32_t(h) & uint32_t(d.point_mask);
-      bool fresh = false;
-      for (int k = 0; k <= d.point_mask; ++k) {
-        int cur = atomicCAS(&d.point_table[probe], -1, int(slot));
-        if (cur == -1) {
-          fresh = true;
-          break;
-        }
-        V2 y = v2(__ldcg(&d.bverts[cur].x), __ldcg(&d.bverts[cur].y));
-        if (y == x && __ldcg(&d.blayers[cur]) == layer) break;
-        probe = (probe + 1) & uint32_t(d.point_mask);
+  }
+}
+
+// Each distinct (layer, point) enters the point hierarchy once: a vertex
+// shared by several patches would otherwise be a candidate of every query
+// several times over.  One thread per boundary vertex inserts it into an
+// open-addressing table keyed by its bits and layer; the first slot to claim
+// an entry adds the point.
+__global__ void k_unique_points(Dev d) {
+  if (d.status[kError] != 0) return;
+  const int total = d.sc[kLiveVertices];
+  for (int64_t slot = tid(); slot < total; slot += stride()) {
+    const V2 x = d.bverts[slot];
+    const int layer = d.blayers[slot];
+    uint64_t h = mix64(mix64(key_bits(x.x)) ^ key_bits(x.y)) ^ mix64(uint64_t(layer) + 7ull);
+    uint32_t probe = uint32_t(h) & uint32_t(d.point_mask);
+    bool fresh = false;
+    for (int k = 0; k <= d.point_mask; ++k) {
+      const int cur = atomicCAS(&d.point_table[probe], -1, int(slot));
+      if (cur == -1) {
+        fresh = true;
+        break;
       }
-      int u = reserve(&d.sc[kUniqueVertices], fresh ? 1 : 0);
-      if (fresh) {
-        d.uverts[u] = x;
-        d.pt_lo[u] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
-                                 float(layer), 0.f);
-        d.pt_hi[u] = make_float4(__double2float_ru(x.x + 2.0e-7), __double2float_ru(x.y + 2.0e-7),
-                                 float(layer), 0.f);
-      }
+      if (d.bverts[cur] == x && d.blayers[cur] == layer) break;
+      probe = (probe + 1) & uint32_t(d.point_mask);
+    }
+    const int u = reserve(&d.sc[kUniqueVertices], fresh ? 1 : 0);
+    if (fresh) {
+      d.uverts[u] = x;
+      d.pt_lo[u] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
+                               float(layer), 0.f);
+      d.pt_hi[u] = make_float4(__double2float_ru(x.x + 2.0e-7), __double2float_ru(x.y + 2.0e-7),
+                               float(layer), 0.f);
     }
   }
 }
@@ -272,7 +278,7 @@ cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStrea
 
 cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
                              cudaStream_t st) {
-  const int64_t R = d.cap.regions;
+  const int64_t R = d.cap.regions, E = d.cap.vertices;
   k_mesh_counts<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
@@ -280,6 +286,8 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   note_launch();
   EDP_CHECK(cudaMemsetAsync(d.point_table, 0xff, sizeof(int) * (int64_t(d.point_mask) + 1), st));
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
+  note_launch();
+  k_unique_points<<<blocks(E), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
   EDP_CHECK(order_polygons(d, true, s, st));

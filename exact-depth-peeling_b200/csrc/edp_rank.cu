@@ -25,10 +25,12 @@ __global__ void k_rank_begin(Dev d) {
   d.sc[kLivePolygons] = int(min(int64_t(d.status[kPolygons]), d.cap.regions));
 }
 
+// counts[k] is the edge count of the k-th polygon in spatial order, so that
+// the patch edges are laid out, matched and connected in that order.
 __global__ void k_polygon_init(Dev d) {
   const int live = live_polygons(d);
   for (int64_t i = tid(); i < live; i += stride()) {
-    d.counts[i] = d.out_n[i];
+    d.counts[i] = d.out_n[d.order[i]];
     d.parents[i] = int(i);
     d.group_counts[i] = 0;
   }
@@ -47,14 +49,15 @@ __global__ void k_check_edges(Dev d) {
 // itself (components.py:287-327).
 __global__ void k_patch_edges(Dev d) {
   const int live = live_polygons(d);
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t o = tid(); o < live; o += stride()) {
     if (d.status[kError] != 0) return;
+    const int i = d.order[o];
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
     const int n = d.out_n[i], source = d.out_src[i];
     const V2 *q = d.src_v + int64_t(kSourceVertices) * source;
     const int qn = d.src_n[source];
     for (int k = 0; k < n; ++k) {
-      int64_t slot = int64_t(d.offsets[i]) + k;
+      int64_t slot = int64_t(d.offsets[o]) + k;
       if (slot >= d.cap.vertices) break;
       V2 a = p[k], b = p[(k + 1) % n];
       unsigned long long owner = 0x8000000000000000ull | static_cast<unsigned>(source);
@@ -74,7 +77,7 @@ __global__ void k_patch_edges(Dev d) {
       d.owners[slot] = owner;
       d.starts[slot] = a;
       d.ends[slot] = b;
-      d.tasks[slot] = make_int2(int(i), k);
+      d.tasks[slot] = make_int2(i, k);
       d.partners[slot] = -1;
     }
   }
@@ -623,6 +626,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   const int64_t R = d.cap.regions, E = d.cap.vertices;
   k_rank_begin<<<1, 1, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(order_polygons(d, false, s, st));
   k_polygon_init<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   const bool connected = d.propagate_ranks || d.merge_regions;
@@ -658,7 +662,6 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
     note_launch();
   }
-  EDP_CHECK(order_polygons(d, false, s, st));
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   k_heavy_hits<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
