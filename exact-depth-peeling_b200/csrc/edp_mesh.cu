@@ -124,7 +124,7 @@ __device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
 // acceptance test and therefore the triangles are the same.
 constexpr int kPolygonSplits = 256;  // split points buffered per polygon
 
-__global__ void __launch_bounds__(kBlock) k_mesh_polygons(Dev d, int edge_capacity) {
+__global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_capacity) {
   const int live = d.sc[kLivePolygons];
   const int leaves = *d.point_tree.size;
   double split_t[kPolygonSplits];
