@@ -119,6 +119,19 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def ncu_traffic(config, kernel="k_mesh_polygons"):
+    """DRAM bytes (read + write) of one launch of `kernel` on this workload, as
+    recorded from an ncu capture in profiles/<kernel>_<config>.md, or None."""
+    path = ROOT / "profiles" / f"{kernel}_{config}.md"
+    try:
+        for line in path.read_text().splitlines():
+            if line.startswith("| dram bytes per launch |"):
+                return int(line.split("|")[2].strip())
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def cpu_baseline(arrays, budget_s=25.0):
     """The reference's CPU path (fast-bvh-peel, restated) on all host threads;
     a bounded sample: one warm-up extraction plus as many timed ones as fit."""
@@ -272,7 +285,9 @@ def run_ours(args, rank, world, local_rank):
     roofline = {
         "bound": "hbm", "kernel": "k_mesh_polygons (noding, fan emission, world lift)",
         "achieved": emit_bytes / (emit_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-        "frac": emit_bytes / (emit_ms * 1e-3) / 1e9 / peak, "traffic": None,
+        "frac": emit_bytes / (emit_ms * 1e-3) / 1e9 / peak,
+        "traffic": ncu_traffic(args.config),
+        "traffic_source": f"ncu capture recorded in profiles/k_mesh_polygons_{args.config}.md",
         "peak_source": f"{peak_kind} copy bandwidth", "algorithmic_bytes": emit_bytes,
         "launch_ms": emit_ms,
         "pipeline": {"bytes_per_mesh": mesh_bytes,
