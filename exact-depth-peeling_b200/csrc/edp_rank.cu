@@ -453,41 +453,67 @@ __global__ void k_ray_hits(Dev d) {
   count_add(&d.metrics[kRayCandidateTests], tests);
 }
 
-__global__ void k_heavy_hits(Dev d) {
+// The continuation of the rays whose primary pass did not finish, one warp
+// per ray (event_kernels.py:248-298).  The warp resumes the walk at the first
+// leaf the primary pass did not reach and walks the rest of the source
+// hierarchy 32 nodes at a time; each lane of a leaf batch takes one candidate,
+// and the batch's hits go to the shared pool with one reservation.  The
+// candidates, and so the hits, are those of the reference's disjoint-subtree
+// continuation.
+__global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
+  const unsigned full = 0xffffffffu;
   if (d.status[kError] != 0) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
   const int leaves = *d.source_tree.size;
   const long long jobs = d.metrics[kHeavyRayGroups];
-  int parts, width;
-  heavy_partition(leaves, jobs, parts, width);
-  long long tests = 0;
-  HitBuffer hits;
-  for (long long task = tid(); task < jobs * parts; task += stride()) {
-    int2 job = d.heavy_queries[task / parts];
-    int part = int(task % parts);
-    int first = leaves + part * width;
-    if (job.y >= first + width) continue;
-    int root = parts + part, node = job.y > first ? job.y : root, end = successor(root);
-    const int i = job.x;
-    V2 x = d.samples[i];
-    float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
-    float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
-    int found = 0;
-    while (node > 0 && node != end) {
-      int s;
-      node = query_next(d.source_tree, leaves, lo, hi, node, end, s);
-      if (s < 0) break;
-      ++tests;
-      if (contains_flat(d, s, x)) {
-        hits.source[hits.count] = s;
-        hits.depth[hits.count] = value(d.scores[s], x);
-        ++found;
-        if (++hits.count == HitBuffer::kSize) hits.flush(d, i);
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  long long tests = 0;  // lane 0's tally
+  for (int64_t j = tid() >> 5; j < jobs; j += warps) {
+    const int2 job = d.heavy_queries[j];
+    const int i = job.x, cursor = job.y - leaves;  // job.y: the first leaf node left
+    const V2 x = d.samples[i];
+    const float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
+    const float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
+    WarpWalk w;
+    walk_begin(w, d.source_tree, leaves, lo, hi, cursor);
+    int budget = 0x7fffffff, first, resume, found = 0;
+    unsigned batch;
+    bool overflow = false;
+    while (walk_next(w, d.source_tree, leaves, lo, hi, cursor, budget, batch, first, resume)) {
+      tests += __popc(batch);
+      bool hit = false;
+      int s = 0;
+      double depth = 0.0;
+      if ((batch >> lane) & 1u) {
+        s = __ldg(&d.source_tree.ids[first + lane]);
+        hit = contains_flat(d, s, x);
+        if (hit) depth = value(d.scores[s], x);
       }
+      const unsigned hits = __ballot_sync(full, hit);
+      if (!hits) continue;
+      const int count = __popc(hits);
+      long long slot = 0;
+      if (lane == 0)
+        slot = static_cast<long long>(atomicAdd(
+            reinterpret_cast<unsigned long long *>(&d.metrics[kRayHits]), (unsigned long long)count));
+      slot = __shfl_sync(full, slot, 0);
+      if (slot + count > d.cap.hits) {
+        overflow = true;
+      } else if (hit) {
+        const long long at = slot + __popc(hits & below);
+        d.hit_depth[at] = depth;
+        d.hit_src[at] = s;
+        d.hit_group[at] = i;
+      }
+      found += count;
     }
-    if (hits.count) hits.flush(d, i);
-    if (found) atomicAdd(&d.group_counts[i], found);
+    if (lane == 0) {
+      if (overflow) set_error(d.status, kErrHits);
+      if (found) atomicAdd(&d.group_counts[i], found);
+    }
   }
-  count_add(&d.metrics[kRayCandidateTests], tests);
+  if (lane == 0) add_metric(d, kRayCandidateTests, tests);
 }
 
 __global__ void k_check_hits(Dev d) {
@@ -664,7 +690,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   }
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
-  k_heavy_hits<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
+  k_heavy_hits<<<148 * 16, kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
   k_check_hits<<<1, 1, 0, st>>>(d);
