@@ -427,7 +427,10 @@ cudaError_t tree_build(TreeBuffers &t, const float4 *lo, const float4 *hi, const
   const unsigned g = grid_for(t.leaves_cap, 256) < 4 * 148 ? grid_for(t.leaves_cap, 256) : 4 * 148;
   k_tree_keys<<<g, 256, 0, st>>>(lo, hi, t.count, t.size, t.keys, t.ids, layered ? 1 : 0);
   note_launch();
-  int bits = layered ? 64 : 30;
+  // Layered keys hold the layer above 30 Morton bits; 48 key bits order them
+  // for up to 65536 layers.  Deeper scenes leave higher layer bits unordered,
+  // which only loosens the hierarchy: any leaf order gives the same queries.
+  int bits = layered ? 48 : 30;
   EDP_CHECK(sort_pairs_u64(t.keys, t.keys_tmp, t.ids, t.ids_tmp, t.count, t.leaves_cap, bits, s, st));
   return tree_refit(t, lo, hi, st);
 }

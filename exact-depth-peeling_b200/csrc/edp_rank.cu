@@ -229,10 +229,15 @@ __device__ inline int cell_of(V2 x) {
 // Identical samples form one query group, whose id is the smallest polygon
 // index in it (the reference groups by sorted position, event_kernels.py:71-92).
 // Each 32x32 image cell also gathers its samples' bounding rectangle as a
-// sharing proposal (beams.py:49-86).
+// sharing proposal (beams.py:49-86).  Samples are taken in spatial order, so
+// the lanes of a warp mostly share cells: lanes with one cell combine their
+// minimum index and rectangle first (exact min / max) and one of them updates
+// the cell.
 __global__ void k_group_insert(Dev d) {
+  namespace cg = cooperative_groups;
   const int live = live_polygons(d);
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t k = tid(); k < live; k += stride()) {
+    const int i = d.order[k];
     V2 x = d.samples[i];
     uint32_t slot = uint32_t(point_key(x)) & uint32_t(d.sample_mask);
     for (int probe = 0; probe <= d.sample_mask; ++probe) {
@@ -243,12 +248,20 @@ __global__ void k_group_insert(Dev d) {
     atomicMin(&d.sample_min[slot], int(i));
     d.sample_slot[i] = int(slot);
     if (d.share_regions) {
-      int c = cell_of(x);
-      atomicMin(&d.cell_min[c], int(i));
-      atomic_min_double(&d.cell_bounds[4 * c + 0], x.x);
-      atomic_min_double(&d.cell_bounds[4 * c + 1], x.y);
-      atomic_max_double(&d.cell_bounds[4 * c + 2], x.x);
-      atomic_max_double(&d.cell_bounds[4 * c + 3], x.y);
+      const int c = cell_of(x);
+      cg::coalesced_group cell = cg::labeled_partition(cg::coalesced_threads(), c);
+      const int first = cg::reduce(cell, i, cg::less<int>());
+      const double lx = cg::reduce(cell, x.x, cg::less<double>());
+      const double ly = cg::reduce(cell, x.y, cg::less<double>());
+      const double hx = cg::reduce(cell, x.x, cg::greater<double>());
+      const double hy = cg::reduce(cell, x.y, cg::greater<double>());
+      if (cell.thread_rank() == 0) {
+        atomicMin(&d.cell_min[c], first);
+        atomic_min_double(&d.cell_bounds[4 * c + 0], lx);
+        atomic_min_double(&d.cell_bounds[4 * c + 1], ly);
+        atomic_max_double(&d.cell_bounds[4 * c + 2], hx);
+        atomic_max_double(&d.cell_bounds[4 * c + 3], hy);
+      }
     }
   }
 }
