@@ -91,10 +91,11 @@ enum Scalar : int {
   kLiveHits = 2,       // min(metrics[5], hits)
   kLiveVertices = 3,   // min(status[6], vertices)
   kSourceCount = 4,    // n (constant)
-  kSegmentCount = 5,   // 8 n (constant)
+  kSegmentCount = 5,   // distinct contour segments (the hierarchy's items)
   kFrontierLive = 6,   // min(status[0], frontier)
   kUniqueVertices = 7, // distinct (layer, point) boundary vertices
   kSortHits = 8,       // hits for the global hit sort: all when a group is large, else 0
+  kSegmentSlots = 9,   // 8 n (constant): candidate contour segment slots
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 16
 };
@@ -131,9 +132,12 @@ struct Dev {
   unsigned long long *edge_keys;  // welded edge key of each face edge (topology owner)
   int ekey_mask;
   // contour segments: kSourceVertices slots per source
-  V2 *seg_a, *seg_b;
+  V2 *slot_a, *slot_b;      // per candidate slot (8 per source): canonical end points
+  int *seg_flag, *seg_pos;  // per slot: representative of its group, its compact index
   double *seg_za, *seg_zb;  // per table slot: minimum endpoint depths
-  V2 *seg_near;             // per representative segment: (near depth a, near depth b)
+  // Distinct segments, compacted in slot order: end points, (near depth a, near
+  // depth b) and boxes; the contour hierarchy is built over these.
+  V2 *seg_a, *seg_b, *seg_near;
   float4 *seg_lo, *seg_hi;
   int *seg_table, *seg_min, *seg_slot;
   int seg_mask;

@@ -18,7 +18,7 @@ __global__ void k_reset(Dev d) {
   if (i < kScalarCount) d.sc[i] = 0;
   if (i == 0) {
     d.sc[kSourceCount] = d.n;
-    d.sc[kSegmentCount] = kSourceVertices * d.n;
+    d.sc[kSegmentSlots] = kSourceVertices * d.n;
     *d.parity = 0;
     *d.condition = 0;
   }
@@ -295,8 +295,8 @@ __global__ void k_segments(Dev d) {
       za = value(sc, a);
       zb = value(sc, b);
       // Publish the endpoints before the slot can be seen by other threads.
-      d.seg_a[i] = a;
-      d.seg_b[i] = b;
+      d.slot_a[i] = a;
+      d.slot_b[i] = b;
       __threadfence();
       uint64_t h = mix64(key_bits(a.x));
       h = mix64(h ^ key_bits(a.y));
@@ -306,8 +306,8 @@ __global__ void k_segments(Dev d) {
       for (int probe = 0; probe <= d.seg_mask; ++probe) {
         int cur = atomicCAS(&d.seg_table[slot], -1, int(i));
         if (cur == -1) break;
-        V2 ca = v2(__ldcg(&d.seg_a[cur].x), __ldcg(&d.seg_a[cur].y));
-        V2 cb = v2(__ldcg(&d.seg_b[cur].x), __ldcg(&d.seg_b[cur].y));
+        V2 ca = v2(__ldcg(&d.slot_a[cur].x), __ldcg(&d.slot_a[cur].y));
+        V2 cb = v2(__ldcg(&d.slot_b[cur].x), __ldcg(&d.slot_b[cur].y));
         if (ca == a && cb == b) break;
         slot = (slot + 1) & uint32_t(d.seg_mask);
       }
@@ -316,30 +316,40 @@ __global__ void k_segments(Dev d) {
       atomic_min_double(&d.seg_zb[slot], zb);
       d.seg_slot[i] = int(slot);
     } else {
-      d.seg_a[i] = a;
-      d.seg_b[i] = b;
+      d.slot_a[i] = a;
+      d.slot_b[i] = b;
     }
   }
 }
 
-__global__ void k_segment_bounds(Dev d) {
+// The first slot of each group represents it (event_kernels.py:440-501).
+__global__ void k_segment_flags(Dev d) {
   const int64_t total = int64_t(kSourceVertices) * d.n;
   for (int64_t i = tid(); i < total; i += stride()) {
-    int slot = d.seg_slot[i];
-    float4 lo = empty_lo(), hi = empty_hi();
-    if (slot >= 0 && d.seg_min[slot] == int(i)) {
-      V2 a = d.seg_a[i], b = d.seg_b[i];
-      double za = d.seg_za[slot], zb = d.seg_zb[slot];
-      d.seg_near[i] = v2(za, zb);
-      double pz = 2.0e-7 * fmax(1.0, fmax(fabs(za), fabs(zb)));
-      lo = make_float4(float(fmin(a.x, b.x) - 2.0e-7), float(fmin(a.y, b.y) - 2.0e-7),
-                       float(fmin(za, zb) - pz), 0.f);
-      hi = make_float4(float(fmax(a.x, b.x) + 2.0e-7), float(fmax(a.y, b.y) + 2.0e-7),
-                       float(fmax(za, zb) + pz), 0.f);
-      atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kUniqueContours]), 1ull);
-    }
-    d.seg_lo[i] = lo;
-    d.seg_hi[i] = hi;
+    const int slot = d.seg_slot[i];
+    const bool first = slot >= 0 && d.seg_min[slot] == int(i);
+    d.seg_flag[i] = first ? 1 : 0;
+    count_add(&d.metrics[kUniqueContours], first ? 1 : 0);
+  }
+}
+
+// Representatives, compacted in slot order (seg_pos is the scan of seg_flag),
+// with their near depths and padded boxes.
+__global__ void k_segment_compact(Dev d) {
+  const int64_t total = int64_t(kSourceVertices) * d.n;
+  for (int64_t i = tid(); i < total; i += stride()) {
+    if (!d.seg_flag[i]) continue;
+    const int c = d.seg_pos[i], slot = d.seg_slot[i];
+    const V2 a = d.slot_a[i], b = d.slot_b[i];
+    const double za = d.seg_za[slot], zb = d.seg_zb[slot];
+    const double pz = 2.0e-7 * fmax(1.0, fmax(fabs(za), fabs(zb)));
+    d.seg_a[c] = a;
+    d.seg_b[c] = b;
+    d.seg_near[c] = v2(za, zb);
+    d.seg_lo[c] = make_float4(float(fmin(a.x, b.x) - 2.0e-7), float(fmin(a.y, b.y) - 2.0e-7),
+                              float(fmin(za, zb) - pz), 0.f);
+    d.seg_hi[c] = make_float4(float(fmax(a.x, b.x) + 2.0e-7), float(fmax(a.y, b.y) + 2.0e-7),
+                              float(fmax(za, zb) + pz), 0.f);
   }
 }
 
@@ -416,10 +426,14 @@ cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree
   if (d.n > 0) {
     k_segments<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();
-    k_segment_bounds<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+    k_segment_flags<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+    note_launch();
+    EDP_CHECK(scan_exclusive(d.seg_flag, d.seg_pos, d.sc + kSegmentSlots, kSourceVertices * d.n,
+                             d.sc + kSegmentCount, s, st));
+    k_segment_compact<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();
   }
-  EDP_CHECK(tree_build(seg_tree, d.seg_lo, d.seg_hi, nullptr, kSourceVertices * d.n, false, s, st));
+  EDP_CHECK(tree_build(seg_tree, d.seg_lo, d.seg_hi, d.sc + kSegmentCount, 0, false, s, st));
   k_seed<<<blocks(d.n), kBlock, 0, st>>>(d);
   note_launch();
   k_loop_condition<<<1, 1, 0, st>>>(d);

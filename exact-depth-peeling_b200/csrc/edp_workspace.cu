@@ -149,6 +149,10 @@ cudaError_t allocate_event(edp_peeler *p) {
                 E = d.cap.vertices, S = int64_t(kSourceVertices) * n;
   EDP_CHECK(allocate_shared(p));
   d.seg_mask = table_mask(S);
+  EDP_CHECK(alloc(p, &d.slot_a, S));
+  EDP_CHECK(alloc(p, &d.slot_b, S));
+  EDP_CHECK(alloc(p, &d.seg_flag, S));
+  EDP_CHECK(alloc(p, &d.seg_pos, S));
   EDP_CHECK(alloc(p, &d.seg_a, S));
   EDP_CHECK(alloc(p, &d.seg_b, S));
   EDP_CHECK(alloc(p, &d.seg_near, S));
@@ -200,7 +204,9 @@ cudaError_t allocate_event(edp_peeler *p) {
   int64_t largest = H;
   for (int64_t v : {p->point_tree.leaves_cap, p->seg_tree.leaves_cap, p->source_tree.leaves_cap, R})
     largest = v > largest ? v : largest;
-  return allocate_scratch(p, largest, R > E ? R : E);
+  int64_t scan = R > E ? R : E;
+  scan = S > scan ? S : scan;  // the segment-slot compaction
+  return allocate_scratch(p, largest, scan);
 }
 
 cudaError_t allocate_device(edp_peeler *p) {
