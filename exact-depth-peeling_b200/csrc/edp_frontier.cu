@@ -212,7 +212,7 @@ __device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int
 // tested against the part's box when they are expanded.  A patch that has
 // met every candidate is final and goes to the output pool; one that spends
 // its budget carries over.  Warps take patches from a shared counter.
-__global__ void __launch_bounds__(kBlock) k_subdivide(Dev d) {
+__global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
   __shared__ V2 s_parts[kWarps][2][kMaxVertices];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   V2 *left_part = s_parts[warp][0], *right_part = s_parts[warp][1];
