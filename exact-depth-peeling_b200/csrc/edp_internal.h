@@ -96,6 +96,7 @@ enum Scalar : int {
   kUniqueVertices = 7, // distinct (layer, point) boundary vertices
   kSortHits = 8,       // hits for the global hit sort: all when a group is large, else 0
   kSegmentSlots = 9,   // 8 n (constant): candidate contour segment slots
+  kMergedLive = 10,    // polygons left after optional convex merging
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 16
 };
@@ -168,6 +169,11 @@ struct Dev {
   unsigned long long *hkeys, *hkeys_tmp;
   int *group_counts, *group_offsets;
   int *group_fill;  // hits placed in each group so far
+  // Optional convex merging: each polygon's chosen patch edge, and the
+  // compaction copy of the outputs (allocated with merge_regions only).
+  int *merge_choice;
+  V2 *merged_v;
+  int *merged_n, *merged_src, *merged_layer;
   // boundary noding and triangles
   V2 *bverts;      // per polygon vertex slot
   int *blayers;

@@ -648,6 +648,109 @@ __global__ void k_assign(Dev d) {
 
 __global__ void k_layers_reset(Dev d) { d.status[kLayers] = 0; }
 
+// ---------------------------------------------------------------- merging
+// Optional convex coalescing (components.py:274-395).  A matched pair of
+// patch edges whose polygons share source and layer proposes a merge when the
+// union stays convex at both joint vertices; every polygon keeps the smallest
+// proposing edge, and a pair merges when both of its polygons chose it.  Each
+// polygon is in at most one merge, so merges never touch the same slot.
+__global__ void k_merge_propose(Dev d) {
+  const int total = d.sc[kPatchEdges];
+  for (int64_t t = tid(); t < total; t += stride()) {
+    if (d.status[kError] != 0) return;
+    const int other = d.partners[t];
+    if (other <= t) continue;
+    const int2 ta = d.tasks[t], tb = d.tasks[other];
+    if (d.out_src[ta.x] != d.out_src[tb.x] || d.out_layer[ta.x] != d.out_layer[tb.x]) continue;
+    const int na = d.out_n[ta.x], nb = d.out_n[tb.x];
+    if (na < 3 || nb < 3 || na + nb - 2 > kMaxVertices) continue;
+    const V2 *a = d.out_v + int64_t(kMaxVertices) * ta.x;
+    const V2 *b = d.out_v + int64_t(kMaxVertices) * tb.x;
+    const V2 u = a[ta.y], v = b[tb.y];
+    if (cross(a[(ta.y + na - 1) % na], u, b[(tb.y + 2) % nb]) >= 0.0 &&
+        cross(b[(tb.y + nb - 1) % nb], v, a[(ta.y + 2) % na]) >= 0.0) {
+      atomicMin(&d.merge_choice[ta.x], int(t));
+      atomicMin(&d.merge_choice[tb.x], int(t));
+    }
+  }
+}
+
+// The joined ring runs over all of a's vertices from the end of the shared
+// edge, then b's vertices but the shared two; exactly collinear vertices are
+// dropped.  The merged polygon replaces a, and b is emptied.
+__global__ void k_merge(Dev d) {
+  const int total = d.sc[kPatchEdges];
+  long long merged = 0;
+  for (int64_t t = tid(); t < total; t += stride()) {
+    if (d.status[kError] != 0) break;
+    const int other = d.partners[t];
+    if (other <= t) continue;
+    const int2 ta = d.tasks[t], tb = d.tasks[other];
+    if (d.merge_choice[ta.x] != t || d.merge_choice[tb.x] != t) continue;
+    V2 *a = d.out_v + int64_t(kMaxVertices) * ta.x;
+    const V2 *b = d.out_v + int64_t(kMaxVertices) * tb.x;
+    const int na = d.out_n[ta.x], nb = d.out_n[tb.x];
+    V2 joined[kMaxVertices];
+    int m = 0;
+    for (int j = 0; j < na; ++j) joined[m++] = a[(ta.y + 1 + j) % na];
+    for (int j = 0; j < nb - 2; ++j) joined[m++] = b[(tb.y + 2 + j) % nb];
+    int kept = 0;
+    V2 q[kMaxVertices];
+    for (int j = 0; j < m; ++j) {
+      const V2 x = joined[j];
+      if (cross(joined[(j + m - 1) % m], x, joined[(j + 1) % m]) != 0.0) q[kept++] = x;
+    }
+    if (kept < 3) continue;
+    for (int j = 0; j < kept; ++j) a[j] = q[j];
+    d.out_n[ta.x] = kept;
+    d.out_n[tb.x] = 0;
+    ++merged;
+  }
+  count_add(&d.metrics[kMergedPolygons], merged);
+}
+
+__global__ void k_merge_counts(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride())
+    d.counts[i] = d.status[kError] == 0 && d.out_n[i] > 0 ? 1 : 0;
+}
+
+// Live polygons, compacted in slot order into the copy and back
+// (components.py:356-395).
+__global__ void k_merge_compact(Dev d) {
+  const int live = live_polygons(d);
+  for (int64_t i = tid(); i < live; i += stride()) {
+    if (d.status[kError] != 0 || d.out_n[i] <= 0) continue;
+    const int slot = d.offsets[i], n = d.out_n[i];
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    V2 *q = d.merged_v + int64_t(kMaxVertices) * slot;
+    for (int j = 0; j < n; ++j) q[j] = p[j];
+    d.merged_n[slot] = n;
+    d.merged_src[slot] = d.out_src[i];
+    d.merged_layer[slot] = d.out_layer[i];
+  }
+}
+
+__global__ void k_merge_restore(Dev d) {
+  if (d.status[kError] != 0) return;
+  const int kept = d.sc[kMergedLive];
+  for (int64_t i = tid(); i < kept; i += stride()) {
+    const int n = d.merged_n[i];
+    const V2 *q = d.merged_v + int64_t(kMaxVertices) * i;
+    V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    for (int j = 0; j < n; ++j) p[j] = q[j];
+    d.out_n[i] = n;
+    d.out_src[i] = d.merged_src[i];
+    d.out_layer[i] = d.merged_layer[i];
+  }
+}
+
+__global__ void k_merge_finish(Dev d) {
+  if (d.status[kError] != 0) return;
+  d.status[kPolygons] = d.sc[kMergedLive];
+  d.sc[kLivePolygons] = d.sc[kMergedLive];
+}
+
 unsigned blocks(int64_t n) {
   int64_t g = ceil_div(n > 0 ? n : 1, kBlock);
   return unsigned(g < 148 * 16 ? g : 148 * 16);
@@ -728,6 +831,22 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   note_launch();
   k_assign<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  if (d.merge_regions) {
+    EDP_CHECK(cudaMemsetAsync(d.merge_choice, 0x7f, sizeof(int) * R, st));
+    k_merge_propose<<<blocks(E), kBlock, 0, st>>>(d);
+    note_launch();
+    k_merge<<<blocks(E), kBlock, 0, st>>>(d);
+    note_launch();
+    k_merge_counts<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
+    EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kMergedLive, s, st));
+    k_merge_compact<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
+    k_merge_restore<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
+    k_merge_finish<<<1, 1, 0, st>>>(d);
+    note_launch();
+  }
   return cudaGetLastError();
 }
 

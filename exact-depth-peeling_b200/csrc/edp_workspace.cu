@@ -190,6 +190,13 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.starts, E));
   EDP_CHECK(alloc(p, &d.ends, E));
   EDP_CHECK(alloc(p, &d.partners, E));
+  if (d.merge_regions) {
+    EDP_CHECK(alloc(p, &d.merge_choice, R));
+    EDP_CHECK(alloc(p, &d.merged_v, R * kMaxVertices));
+    EDP_CHECK(alloc(p, &d.merged_n, R));
+    EDP_CHECK(alloc(p, &d.merged_src, R));
+    EDP_CHECK(alloc(p, &d.merged_layer, R));
+  }
   d.edge_hash_mask = table_mask(E);
   EDP_CHECK(alloc(p, &d.edge_hash, int64_t(d.edge_hash_mask) + 1));
   EDP_CHECK(alloc(p, &d.hit_depth, H));

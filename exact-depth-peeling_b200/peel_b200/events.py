@@ -66,8 +66,6 @@ class EventPeeler(_Peeler):
             raise ValueError("Capacities must be positive; edge_vertices must be <= 128")
         if layers < 0 or layers > ec.layers:
             raise ValueError("layers must be zero (all), or fit in the layer capacity")
-        if merge_regions:
-            raise ValueError("merge_regions is not available in this build")
         self.event_cap = ec
         self.cap = ec
         self.share_regions = share_regions
