@@ -306,6 +306,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": None, "clocks": clocks.summary(),
         "stages_ms": stage_ms,
         "output": {k: check[k] for k in ("polygons", "triangles", "layers", "boundary_vertices")},
+        "throughput": {"fragments_per_s": check["polygons"] / (ms_per_mesh * 1e-3),
+                       "triangles_per_s": check["triangles"] / (ms_per_mesh * 1e-3)},
         "capacities": vars(capacities),
     }
     outside = np.zeros(2, dtype=np.int64)
