@@ -45,6 +45,22 @@ def scene_arrays(data):
     return vertices, faces, camera, settings, labels
 
 
+def scene_data(vertices, faces, camera, settings):
+    """Scene JSON (as a dict) of host or device arrays: the inverse of
+    ``scene_arrays``, one triangle per face with id = face index.  Binary64
+    values are written as JSON numbers, whose shortest repr reads back exactly."""
+    host = [np.asarray(a.cpu() if hasattr(a, "cpu") else a) for a in
+            (vertices, faces, camera, settings)]
+    v, f, cam, st = host
+    tri = v[f.astype(np.int64)]
+    return {
+        "window": [float(x) for x in st[:4]],
+        "camera": {"type": "perspective" if st[4] else "orthographic", "near": float(st[5]),
+                   "world_to_camera": cam[:3].tolist()},
+        "triangles": [{"id": i, "vertices": tri[i].tolist()} for i in range(len(tri))],
+    }
+
+
 def load_scene(path, device="cuda:0"):
     """Upload a scene JSON; returns ([vertices, faces, camera, settings], labels, data)."""
     import torch
