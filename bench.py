@@ -34,16 +34,21 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
 
+DESCRIPTIONS = {
+    "knot-65536": "(3,7) torus-knot tube, 256 rings x 128 segments = 65,536 faces, radius "
+                  "0.3 with N(0,0.02) noise (seed 2), pinhole 60 deg at 3x bounding radius",
+    "icospheres-2560": "two nested noisy icospheres, 2 x 1,280 faces, orthographic",
+    "stack-65536": "65,536 identical-footprint triangles at z = i*1e-3, orthographic",
+    "primitives-720k": "40 noisy spheres and tori (radii log-uniform in [0.05, 0.5], seed 7) "
+                       "packed disjointly, 720,916 faces, pinhole 60 deg",
+    "batched-128": "one graph replay of 128 extractions: 64 turntable pinhole views "
+                   "(seed 5) of a 16,152-face displaced genus-3 surface plus 64 packed-"
+                   "primitive meshes of 1K-32K faces (seed 6)",
+}
+
+
 def workload_config(name, vertices, faces):
-    descriptions = {
-        "knot-65536": "(3,7) torus-knot tube, 256 rings x 128 segments = 65,536 faces, radius "
-                      "0.3 with N(0,0.02) noise (seed 2), pinhole 60 deg at 3x bounding radius",
-        "icospheres-2560": "two nested noisy icospheres, 2 x 1,280 faces, orthographic",
-        "stack-65536": "65,536 identical-footprint triangles at z = i*1e-3, orthographic",
-        "primitives-720k": "40 noisy spheres and tori (radii log-uniform in [0.05, 0.5], seed 7) "
-                           "packed disjointly, 720,916 faces, pinhole 60 deg",
-    }
-    return {"workload": f"{name}: {descriptions.get(name, name)}", "faces": int(len(faces)),
+    return {"workload": f"{name}: {DESCRIPTIONS.get(name, name)}", "faces": int(len(faces)),
             "vertices": int(len(vertices)),
             "l2": "flushed between timed replays (256 MiB device write)",
             "parallelism": "replicas"}
@@ -161,11 +166,25 @@ def run_reference(args, rank, world):
 
     arrays = scenes.CONFIGS[args.config]()
     threads = fastpeel.max_threads()
-    vertices, faces, camera, settings = arrays
-    fastpeel.run(vertices, faces, camera, settings, threads=threads, repeat=max(1, args.warmup))
-    times, info = fastpeel.run(vertices, faces, camera, settings, threads=threads,
-                               repeat=args.steps)
-    ms = 1000.0 * sum(times) / len(times)
+    if isinstance(arrays, list):  # a batch: a bounded sample, 4 views and 4 meshes
+        sample = arrays[:4] + arrays[len(arrays) // 2:len(arrays) // 2 + 4]
+        for v, f, c, st in sample[:1]:
+            fastpeel.run(v, f, c, st, threads=threads, repeat=1)
+        times, layers, triangles = [], 0, 0
+        for v, f, c, st in sample:
+            t, info = fastpeel.run(v, f, c, st, threads=threads, repeat=max(1, args.steps // 4))
+            times.append(sum(t) / len(t))
+            layers, triangles = max(layers, info["layers"]), triangles + info["triangles"]
+        ms = 1000.0 * sum(times) / len(times)
+        info = {"layers": layers, "triangles": triangles}
+        vertices, faces = arrays[0][0], arrays[0][1]
+    else:
+        vertices, faces, camera, settings = arrays
+        fastpeel.run(vertices, faces, camera, settings, threads=threads,
+                     repeat=max(1, args.warmup))
+        times, info = fastpeel.run(vertices, faces, camera, settings, threads=threads,
+                                   repeat=args.steps)
+        ms = 1000.0 * sum(times) / len(times)
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -176,6 +195,124 @@ def run_reference(args, rank, world):
                                    f"warm-up; {info['layers']} layers, {info['triangles']} "
                                    "triangles"},
         "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batched(args, rank, world, local_rank):
+    """The batched configuration: every scene of the batch in one graph replay
+    per step; value = device ms per mesh (batch time / scenes)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from peel_b200 import BatchPeeler, _lib, scenes
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    host = scenes.CONFIGS[args.config]()
+    arrays = [scenes.to_device(h, device) for h in host]
+    batch = BatchPeeler(arrays, fit=True)
+    batch.capture()
+    meshes = len(batch)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        batch.run()
+    batch.read_status()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(batch.stream):
+                flush.zero_()
+                starts[k].record(batch.stream)
+            batch.run()
+            ends[k].record(batch.stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([total], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total = float(t.item())
+    ms_per_step = total / args.steps
+    infos = batch.read_status()
+    triangles = sum(i["triangles"] for i in infos)
+    polygons = sum(i["polygons"] for i in infos)
+
+    # End to end: every scene's inputs uploaded from pinned host memory, the
+    # batch replayed, every status and triangle read back.
+    pinned = [[torch.as_tensor(np.ascontiguousarray(a)).pin_memory() for a in h] for h in host]
+    e2e_steps = 0 if args.quick else max(1, min(args.steps, 3))
+    names = ("triangles_uv", "triangles_world", "triangle_sources", "triangle_layers")
+    d2h = [{n: torch.empty(tuple(getattr(p, n)[:i["triangles"]].shape),
+                           dtype=getattr(p, n).dtype).pin_memory() for n in names}
+           for p, i in zip(batch.peelers, infos)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(batch.stream):
+            for dst, src in zip(arrays, pinned):
+                for d, s_ in zip(dst, src):
+                    d.copy_(s_.reshape(d.shape), non_blocking=True)
+        batch.run()
+        got = batch.read_status()
+        with torch.cuda.stream(batch.stream):
+            for p, i, bufs in zip(batch.peelers, got, d2h):
+                for n, buf in bufs.items():
+                    buf[:i["triangles"]].copy_(getattr(p, n)[:i["triangles"]], non_blocking=True)
+        batch.stream.synchronize()
+    e2e_ms = 1000.0 * (time.perf_counter() - t0) / max(e2e_steps, 1)
+    if rank != 0:
+        return
+    h2d = sum(a.numel() * a.element_size() for h in pinned for a in h)
+    peak, peak_kind = hbm_peak()
+    mesh_bytes = sum(algorithmic_bytes(len(h[0]), len(h[1]), i["triangles"])
+                     for h, i in zip(host, infos))
+    lib = _lib.load()
+    launches = 0
+    for p, i in zip(batch.peelers, infos):
+        outside = np.zeros(2, dtype=np.int64)
+        _lib.check(lib.edp_graph_kernels(p._ws.handle, outside.ctypes.data,
+                                         outside.ctypes.data + 8), "graph kernels")
+        launches += int(outside[0] + outside[1] * i["rounds"])
+    cpu = None
+    if world == 1 and not args.quick:
+        from oracle import fastpeel
+
+        threads = fastpeel.max_threads()
+        sample = host[:2] + host[meshes // 2:meshes // 2 + 2]
+        times = [fastpeel.run(*h, threads=threads, repeat=1)[0][0] for h in sample]
+        cpu = {"value": 1000.0 * sum(times) / len(times), "unit": UNIT, "cores": threads,
+               "kind": "port", "sample": "2 views and 2 meshes of the batch, one extraction "
+                                         "each, mean per mesh; excludes import and projection"}
+    line = {
+        "metric": METRIC, "value": ms_per_step / (meshes * world), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {DESCRIPTIONS[args.config]}", "meshes": meshes,
+                   "faces": int(sum(len(h[1]) for h in host)),
+                   "l2": "flushed between timed replays (256 MiB device write)",
+                   "parallelism": "replicas"},
+        "roofline": {"bound": "hbm", "kernel": "whole batch graph (compulsory bytes)",
+                     "achieved": mesh_bytes / (ms_per_step * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": mesh_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+                     "traffic": None, "peak_source": f"{peak_kind} copy bandwidth",
+                     "algorithmic_bytes": mesh_bytes},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms / meshes if e2e_steps else None, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step":
+                    int(sum(64 + 152 + 128 * i["triangles"] for i in infos))},
+        "gpu_launches": int(args.steps * launches), "clocks": clocks.summary(),
+        "output": {"polygons": polygons, "triangles": triangles,
+                   "layers_max": max(i["layers"] for i in infos)},
+        "throughput": {"fragments_per_s": polygons / (ms_per_step * 1e-3),
+                       "triangles_per_s": triangles / (ms_per_step * 1e-3)},
     }
     print(json.dumps(line), flush=True)
 
@@ -345,7 +482,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.config.startswith("batched"):
+            run_batched(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

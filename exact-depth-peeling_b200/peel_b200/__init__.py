@@ -2,7 +2,8 @@
 ``warp_peel`` call surface: ``DevicePeeler``, ``EventPeeler``,
 ``Capacities``, ``EventCapacities`` (warp_peel/__init__.py:3-6)."""
 
+from .batch import BatchPeeler
 from .events import EventCapacities, EventPeeler
 from .solver import Capacities, DevicePeeler
 
-__all__ = ["Capacities", "DevicePeeler", "EventCapacities", "EventPeeler"]
+__all__ = ["BatchPeeler", "Capacities", "DevicePeeler", "EventCapacities", "EventPeeler"]

@@ -256,6 +256,120 @@ def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7):
     return vertices, faces, camera, settings
 
 
+def marching_tetrahedra(field, lo, hi, cells):
+    """Closed triangle mesh of the zero set of ``field`` (negative inside) over
+    the box [lo, hi] split into ``cells`` grid cells per axis, each cell cut
+    into six tetrahedra around its main diagonal.  A vertex is made once per
+    crossed grid edge (shared by every tetrahedron on the edge), so the mesh is
+    watertight; triangles face the positive side."""
+    lo, hi, cells = np.asarray(lo, float), np.asarray(hi, float), np.asarray(cells, int)
+    axes = [np.linspace(lo[a], hi[a], cells[a] + 1) for a in range(3)]
+    points = np.stack(np.meshgrid(*axes, indexing="ij"), -1)
+    values = field(points)
+    values = np.where(values == 0.0, 1e-12, values)  # no grid point on the surface
+    shape = values.shape
+    flat_p, flat_f = points.reshape(-1, 3), values.reshape(-1)
+    ci, cj, ck = (a.ravel() for a in np.meshgrid(*(np.arange(c) for c in cells), indexing="ij"))
+    index = lambda d: ((ci + d[0]) * shape[1] + cj + d[1]) * shape[2] + ck + d[2]
+    unit = np.eye(3, dtype=int)
+    tets = []
+    for order in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        corner = [np.zeros(3, int)]
+        for axis in order:
+            corner.append(corner[-1] + unit[axis])
+        tets.append(np.stack([index(c) for c in corner], 1))
+    tets = np.concatenate(tets)
+    inside = flat_f[tets] < 0
+    crossing = (inside.sum(1) > 0) & (inside.sum(1) < 4)
+    tets, inside = tets[crossing], inside[crossing]
+    vertex_of, vertices, faces = {}, [], []
+
+    def vertex(a, b):
+        key = (a, b) if a < b else (b, a)
+        if key not in vertex_of:
+            t = flat_f[key[0]] / (flat_f[key[0]] - flat_f[key[1]])
+            vertices.append(flat_p[key[0]] + t * (flat_p[key[1]] - flat_p[key[0]]))
+            vertex_of[key] = len(vertices) - 1
+        return vertex_of[key]
+
+    for tet, flags in zip(tets, inside):
+        ins = [v for v, f in zip(tet, flags) if f]
+        out = [v for v, f in zip(tet, flags) if not f]
+        if len(ins) == 1 or len(out) == 1:
+            lone, rest = (ins[0], out) if len(ins) == 1 else (out[0], ins)
+            polys = [[vertex(lone, r) for r in rest]]
+        else:
+            a, b = vertex(ins[0], out[0]), vertex(ins[0], out[1])
+            c, d = vertex(ins[1], out[1]), vertex(ins[1], out[0])
+            polys = [[a, b, c], [a, c, d]]
+        outward = flat_p[out].mean(0) - flat_p[ins].mean(0)
+        for tri in polys:
+            pa, pb, pc = (vertices[k] for k in tri)
+            if np.dot(np.cross(pb - pa, pc - pa), outward) < 0:
+                tri = [tri[0], tri[2], tri[1]]
+            faces.append(tri)
+    return np.array(vertices), np.array(faces, dtype=np.int32)
+
+
+def genus3_surface(cells=49, seed=4, amplitude=0.03):
+    """Closed genus-3 surface of about 16K faces (16,152 at the defaults): the
+    union of three tori whose centre circles touch in a row (the thickened
+    chain of circles has three independent loops), its implicit field displaced
+    by a seeded sum of smooth sinusoids, polygonised by marching tetrahedra.
+    An implicit surface does not intersect itself."""
+    rng = np.random.default_rng(seed)
+    major, minor = 1.0, 0.36
+    waves = [(rng.normal(size=3) * 2.0, rng.uniform(0, 2 * np.pi)) for _ in range(4)]
+
+    def field(p):
+        value = np.full(p.shape[:-1], np.inf)
+        for cx in (-2 * major, 0.0, 2 * major):
+            q = p - np.array([cx, 0.0, 0.0])
+            torus_ = np.hypot(np.hypot(q[..., 0], q[..., 1]) - major, q[..., 2]) - minor
+            value = np.minimum(value, torus_)
+        for k, phase in waves:
+            value = value + amplitude / len(waves) * np.sin(p @ k + phase)
+        return value
+
+    pad = minor + amplitude + 0.05
+    hi = np.array([3 * major + pad, major + pad, pad])
+    lo = -hi
+    size = hi - lo
+    counts = np.maximum(1, np.round(size / (size[0] / cells)).astype(int))
+    return marching_tetrahedra(field, lo, hi, counts)
+
+
+def turntable_views(vertices, count=64, seed=5, fov_degrees=60.0):
+    """``count`` pinhole cameras at 3x the bounding radius around the centroid:
+    azimuth uniform in [0, 2 pi), elevation uniform in [-30, 30] degrees."""
+    rng = np.random.default_rng(seed)
+    centroid = vertices.mean(0)
+    bound = np.linalg.norm(vertices - centroid, axis=1).max()
+    views = []
+    for azimuth, elevation in zip(rng.uniform(0, 2 * np.pi, count),
+                                  np.radians(rng.uniform(-30, 30, count))):
+        direction = np.array([np.cos(elevation) * np.cos(azimuth), np.sin(elevation),
+                              np.cos(elevation) * np.sin(azimuth)])
+        views.append(_pinhole(centroid + 3 * bound * direction, centroid, fov_degrees,
+                              near=0.01 * bound))
+    return views
+
+
+def batched_scenes(views=64, meshes=64, seed=6):
+    """The batched workload: ``views`` turntable views of the genus-3 surface,
+    then ``meshes`` packed-primitive meshes of 1K to 32K faces (log-uniform
+    counts, 1 to 4 primitives each).  A list of (vertices, faces, camera,
+    settings)."""
+    vertices, faces = genus3_surface()
+    out = [(vertices, faces, camera, settings)
+           for camera, settings in turntable_views(vertices, views)]
+    rng = np.random.default_rng(seed)
+    for k in range(meshes):
+        total = int(np.exp(rng.uniform(np.log(1024), np.log(32768))))
+        out.append(packed_primitives(total, int(rng.integers(1, 5)), seed=1000 + k))
+    return out
+
+
 def _random_rotation(rng):
     q = rng.normal(size=4)
     q /= np.linalg.norm(q)
@@ -270,6 +384,7 @@ CONFIGS = {
     "icospheres-2560": nested_icospheres,
     "knot-65536": knot_tube,
     "stack-65536": lambda: stress_stack(65536, 0.0),
+    "batched-128": batched_scenes,  # a list of scenes, peeled by one graph replay
 }
 
 
