@@ -157,7 +157,10 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
       if (j < 0) break;
       const V2 x = d.uverts[j];
       for (int e = 0; e < n; ++e) {
-        const V2 a = p[e], b = p[(e + 1) % n], dir = b - a;
+        const V2 a = p[e], b = p[(e + 1) % n];
+        // An edge's own end point has parameter 0 or 1 exactly: never a split.
+        if (x == a || x == b) continue;
+        const V2 dir = b - a;
         const double length2 = dot(dir, dir);
         if (!(length2 > 0.0)) continue;
         // Division-free rejection of points off the edge's line (4x slack over
