@@ -234,7 +234,8 @@ cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaS
 // centre, below the layer when `layered`.
 cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStream_t st);
 
-// Stage launchers (edp_kernels.cu).  Each enqueues kernels on `st`.
+// Stage launchers (edp_prepare.cu, edp_frontier.cu, edp_rank.cu, edp_mesh.cu).  Each
+// enqueues kernels on `st`.
 cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
                           TreeBuffers &seg_tree, cudaStream_t st);
 cudaError_t stage_step(const Dev &d, cudaStream_t st);
