@@ -12,10 +12,13 @@ constexpr int kMaxEdgeVertices = 128;  // edge noding capacity (solver.py:140-14
 __device__ inline int64_t tid() { return blockIdx.x * int64_t(blockDim.x) + threadIdx.x; }
 __device__ inline int64_t stride() { return int64_t(gridDim.x) * blockDim.x; }
 
+// Boundary vertex slots follow the polygons' (layer, Morton) order, so the
+// copies of one point, which neighbouring polygons share, meet the point table
+// close together in time.
 __global__ void k_mesh_counts(Dev d) {
   const int live = d.sc[kLivePolygons];
-  for (int64_t i = tid(); i < live; i += stride())
-    d.counts[i] = d.status[kError] == 0 ? d.out_n[i] : 0;
+  for (int64_t k = tid(); k < live; k += stride())
+    d.counts[k] = d.status[kError] == 0 ? d.out_n[d.order[k]] : 0;
 }
 
 __global__ void k_mesh_check(Dev d) {
@@ -32,11 +35,12 @@ __global__ void k_mesh_check(Dev d) {
 // (kernels.py:953-991, event_kernels.py:504-516).
 __global__ void k_scatter(Dev d) {
   const int live = d.sc[kLivePolygons];
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
+    const int i = d.order[k];
     const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
     const int layer = d.out_layer[i];
-    const int64_t base = d.offsets[i];
+    const int64_t base = d.offsets[k];
     const int n = int(min(int64_t(d.out_n[i]), d.cap.vertices - base));
     for (int j = 0; j < n; ++j) {
       d.bverts[base + j] = p[j];
@@ -282,6 +286,7 @@ cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStrea
 cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
                              cudaStream_t st) {
   const int64_t R = d.cap.regions, E = d.cap.vertices;
+  EDP_CHECK(order_polygons(d, true, s, st));
   k_mesh_counts<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kLiveVertices, s, st));
@@ -293,7 +298,6 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   k_unique_points<<<blocks(E), kBlock, 0, st>>>(d);
   note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
-  EDP_CHECK(order_polygons(d, true, s, st));
   return cudaGetLastError();
 }
 
