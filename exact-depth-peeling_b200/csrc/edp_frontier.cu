@@ -25,7 +25,11 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
   const double z = value(score, p);
   double lx = mine ? p.x : 1.0e30, ly = mine ? p.y : 1.0e30, lz = mine ? z : 1.0e30;
   double hx = mine ? p.x : -1.0e30, hy = mine ? p.y : -1.0e30, hz = mine ? z : -1.0e30;
-  for (int off = 16; off > 0; off >>= 1) {
+  // Lanes [0, width) hold every vertex; a butterfly over them leaves the
+  // result in lane 0, which every lane then reads.
+  int width = 1;
+  while (width < n) width <<= 1;
+  for (int off = width >> 1; off > 0; off >>= 1) {
     lx = fmin(lx, __shfl_xor_sync(kFull, lx, off));
     ly = fmin(ly, __shfl_xor_sync(kFull, ly, off));
     lz = fmin(lz, __shfl_xor_sync(kFull, lz, off));
@@ -33,6 +37,12 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
     hy = fmax(hy, __shfl_xor_sync(kFull, hy, off));
     hz = fmax(hz, __shfl_xor_sync(kFull, hz, off));
   }
+  lx = __shfl_sync(kFull, lx, 0);
+  ly = __shfl_sync(kFull, ly, 0);
+  lz = __shfl_sync(kFull, lz, 0);
+  hx = __shfl_sync(kFull, hx, 0);
+  hy = __shfl_sync(kFull, hy, 0);
+  hz = __shfl_sync(kFull, hz, 0);
   double pz = 2.0e-7 * fmax(1.0, fmax(fabs(lz), fabs(hz)));
   lo = make_float4(float(lx - 2.0e-7), float(ly - 2.0e-7), float(lz - pz), 0.f);
   hi = make_float4(float(hx + 2.0e-7), float(hy + 2.0e-7), float(hz + pz), 0.f);
