@@ -14,6 +14,10 @@ constexpr unsigned kFull = 0xffffffffu;
 // patch takes: every patch meets its candidates in leaf order in any case.
 constexpr int kStepBudget = 48;
 
+// The smallest power of two holding n lanes: a butterfly over it reduces
+// lanes [0, n), the lanes that hold a patch's vertices.
+__device__ inline int lane_width(int n) { return n <= 1 ? 1 : 1 << (32 - __clz(n - 1)); }
+
 __device__ inline V2 shfl(V2 x, int lane) {
   return v2(__shfl_sync(kFull, x.x, lane), __shfl_sync(kFull, x.y, lane));
 }
@@ -27,8 +31,7 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
   double hx = mine ? p.x : -1.0e30, hy = mine ? p.y : -1.0e30, hz = mine ? z : -1.0e30;
   // Lanes [0, width) hold every vertex; a butterfly over them leaves the
   // result in lane 0, which every lane then reads.
-  int width = 1;
-  while (width < n) width <<= 1;
+  const int width = lane_width(n);
   for (int off = width >> 1; off > 0; off >>= 1) {
     lx = fmin(lx, __shfl_xor_sync(kFull, lx, off));
     ly = fmin(ly, __shfl_xor_sync(kFull, ly, off));
@@ -71,6 +74,7 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
                                 const Plane &sc, V2 &a, V2 &b) {
   const int lane = threadIdx.x & 31;
   const bool mine = lane < n;
+  const int width = lane_width(n);
   V2 ca = v2(0.0, 0.0), cb = ca, cn = ca;
   if ((batch >> lane) & 1u) {
     const int c = __ldg(&g.ids[first + lane]);
@@ -94,10 +98,12 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
     const double r = da / (da - db);
     double low = mine && da < 0.0 ? fmax(0.0, r) : 0.0;
     double high = mine && db < 0.0 ? fmin(1.0, r) : 1.0;
-    for (int off = 16; off > 0; off >>= 1) {
+    for (int off = width >> 1; off > 0; off >>= 1) {  // lanes [0, width) hold the edges
       low = fmax(low, __shfl_xor_sync(kFull, low, off));
       high = fmin(high, __shfl_xor_sync(kFull, high, off));
     }
+    low = __shfl_sync(kFull, low, 0);
+    high = __shfl_sync(kFull, high, 0);
     const double rz = za / (za - zb);
     if (za < 0.0) low = fmax(low, rz);
     if (zb < 0.0) high = fmin(high, rz);
