@@ -97,6 +97,9 @@ enum Scalar : int {
   kSortHits = 8,       // hits for the global hit sort: all when a group is large, else 0
   kSegmentSlots = 9,   // 8 n (constant): candidate contour segment slots
   kMergedLive = 10,    // polygons left after optional convex merging
+  kGridOn = 11,        // 1 when the point grid holds every layer of this extraction
+  kGridCells = 12,     // grid cells in use: layers x G^2 when the grid is on, else 0
+  kTreePoints = 13,    // points of the point hierarchy: 0 when the grid is on
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 16
 };
@@ -180,6 +183,12 @@ struct Dev {
   V2 *uverts;      // distinct (layer, point) vertices, indexed by the point hierarchy
   int *point_table;
   int point_mask;
+  // Layered point grid: G x G cells per layer over the unit window for up to
+  // grid_layers layers; cell_start is the exclusive scan of the per-cell point
+  // counts (with the total at the end) and grid_pts the points by cell.
+  int grid_size, grid_layers;
+  int *cell_count, *cell_start;
+  V2 *grid_pts;
   float4 *pt_lo, *pt_hi;
   // A processing order of the live output polygons by the Morton code of
   // their box centre (optionally below the layer), rebuilt by each stage that

@@ -49,6 +49,41 @@ __global__ void k_scatter(Dev d) {
   }
 }
 
+// Grid column (or row) of a window coordinate: floor(v G) clamped to the
+// grid.  Monotone in v, so a query interval's cells hold every point inside it.
+__device__ inline int grid_cell(double v, int g) {
+  const double c = floor(v * double(g));
+  return c < 0.0 ? 0 : c > double(g - 1) ? g - 1 : int(c);
+}
+
+// The grid serves this extraction when it has a row for every layer;
+// otherwise the point hierarchy does.
+__global__ void k_grid_begin(Dev d) {
+  const int layers = d.status[kLayers];
+  const bool on = d.status[kError] == 0 && layers <= d.grid_layers;
+  d.sc[kGridOn] = on ? 1 : 0;
+  d.sc[kGridCells] = on ? int(int64_t(layers) * d.grid_size * d.grid_size) : 0;
+}
+
+__global__ void k_tree_points(Dev d) {
+  d.sc[kTreePoints] = d.sc[kGridOn] ? 0 : d.sc[kUniqueVertices];
+}
+
+// Counting sort of the distinct points by (layer, cell): the scan of the
+// counts gives each cell's start, and each point takes a slot of its cell.
+__global__ void k_grid_scatter(Dev d) {
+  if (!d.sc[kGridOn] || d.status[kError] != 0) return;
+  const int total = d.sc[kUniqueVertices], g = d.grid_size;
+  if (tid() == 0) d.cell_start[d.sc[kGridCells]] = total;
+  for (int64_t u = tid(); u < total; u += stride()) {
+    const V2 x = d.uverts[u];
+    const int layer = int(d.pt_lo[u].z);
+    const int64_t cell = (int64_t(layer) * g + grid_cell(x.y, g)) * g + grid_cell(x.x, g);
+    const int slot = atomicSub(&d.cell_count[cell], 1) - 1;
+    d.grid_pts[d.cell_start[cell] + slot] = x;
+  }
+}
+
 // Each distinct (layer, point) enters the point hierarchy once: a vertex
 // shared by several patches would otherwise be a candidate of every query
 // several times over.  One thread per boundary vertex inserts it into an
@@ -73,6 +108,10 @@ __global__ void k_unique_points(Dev d) {
       probe = (probe + 1) & uint32_t(d.point_mask);
     }
     const int u = reserve(&d.sc[kUniqueVertices], fresh ? 1 : 0);
+    if (fresh && d.sc[kGridOn]) {
+      const int g = d.grid_size;
+      atomicAdd(&d.cell_count[(int64_t(layer) * g + grid_cell(x.y, g)) * g + grid_cell(x.x, g)], 1);
+    }
     if (fresh) {
       d.uverts[u] = x;
       d.pt_lo[u] = make_float4(__double2float_rd(x.x - 2.0e-7), __double2float_rd(x.y - 2.0e-7),
@@ -154,12 +193,9 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
     int count = 0, per_edge[kMaxVertices];
     for (int e = 0; e < n; ++e) per_edge[e] = 0;
     bool overflow = false;
-    int node = 1;
-    while (node > 0 && !overflow) {
-      int j;
-      node = query_next(d.point_tree, leaves, lo, hi, node, 0, j);
-      if (j < 0) break;
-      const V2 x = d.uverts[j];
+    // Test one candidate point against every edge: a split point lies on the
+    // edge's line within EPS, strictly inside the edge.
+    auto node_point = [&](const V2 x) {
       for (int e = 0; e < n; ++e) {
         const V2 a = p[e], b = p[(e + 1) % n];
         // An edge's own end point has parameter 0 or 1 exactly: never a split.
@@ -175,12 +211,36 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
         if (tt > kEps && tt < 1.0 - kEps && fabs(cross(a, b, x)) <= kEps * sqrt(length2)) {
           if (++per_edge[e] > edge_capacity || count == kPolygonSplits) {
             overflow = true;
-            break;
+            return;
           }
           split_t[count] = tt;
           split_edge[count] = (unsigned char)e;
           ++count;
         }
+      }
+    };
+    if (d.sc[kGridOn]) {
+      // The grid cells meeting the polygon's box grown by 1e-9 hold every
+      // same-layer point within 1e-10 of its boundary, hence every split point.
+      const int g = d.grid_size;
+      const double qlx = lx - 1.0e-9, qly = ly - 1.0e-9, qhx = hx + 1.0e-9, qhy = hy + 1.0e-9;
+      const int cx0 = grid_cell(qlx, g), cx1 = grid_cell(qhx, g);
+      for (int cy = grid_cell(qly, g); cy <= grid_cell(qhy, g) && !overflow; ++cy) {
+        const int64_t row = (int64_t(layer) * g + cy) * g;
+        const int end = d.cell_start[row + cx1 + 1];
+        for (int j = d.cell_start[row + cx0]; j < end && !overflow; ++j) {
+          const V2 x = d.grid_pts[j];
+          if (x.x < qlx || x.x > qhx || x.y < qly || x.y > qhy) continue;
+          node_point(x);
+        }
+      }
+    } else {
+      int node = 1;
+      while (node > 0 && !overflow) {
+        int j;
+        node = query_next(d.point_tree, leaves, lo, hi, node, 0, j);
+        if (j < 0) break;
+        node_point(d.uverts[j]);
       }
     }
     if (overflow) {
@@ -293,11 +353,20 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   k_mesh_check<<<1, 1, 0, st>>>(d);
   note_launch();
   EDP_CHECK(cudaMemsetAsync(d.point_table, 0xff, sizeof(int) * (int64_t(d.point_mask) + 1), st));
+  const int64_t cells = int64_t(d.grid_layers) * d.grid_size * d.grid_size;
+  EDP_CHECK(cudaMemsetAsync(d.cell_count, 0, sizeof(int) * cells, st));
+  k_grid_begin<<<1, 1, 0, st>>>(d);
+  note_launch();
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   k_unique_points<<<blocks(E), kBlock, 0, st>>>(d);
   note_launch();
-  EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kUniqueVertices, 0, true, s, st));
+  EDP_CHECK(scan_exclusive(d.cell_count, d.cell_start, d.sc + kGridCells, cells, nullptr, s, st));
+  k_grid_scatter<<<blocks(E), kBlock, 0, st>>>(d);
+  note_launch();
+  k_tree_points<<<1, 1, 0, st>>>(d);
+  note_launch();
+  EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kTreePoints, 0, true, s, st));
   return cudaGetLastError();
 }
 

@@ -7,6 +7,9 @@
 #include "../../include/edp.h"
 #include "edp_internal.h"
 
+#include <algorithm>
+#include <cmath>
+
 using namespace edp;
 
 namespace {
@@ -121,6 +124,18 @@ cudaError_t allocate_shared(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.uverts, E));
   d.point_mask = table_mask(E);
   EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
+  // About sqrt(N) / 1.5 cells per axis (a power of two in [32, 512]), rows for
+  // as many layers as 16M cells allow.
+  {
+    int g = 32;
+    while (g < 512 && double(2 * g) * 1.5 <= std::sqrt(double(n > 0 ? n : 1))) g *= 2;
+    d.grid_size = g;
+    const int64_t per_layer = int64_t(g) * g, budget = int64_t(1) << 24;
+    d.grid_layers = int(std::min<int64_t>(d.cap.layers, std::max<int64_t>(1, budget / per_layer)));
+    EDP_CHECK(alloc(p, &d.cell_count, d.grid_layers * per_layer));
+    EDP_CHECK(alloc(p, &d.cell_start, d.grid_layers * per_layer + 1));
+    EDP_CHECK(alloc(p, &d.grid_pts, E));
+  }
   EDP_CHECK(alloc(p, &d.pt_lo, E));
   EDP_CHECK(alloc(p, &d.pt_hi, E));
   EDP_CHECK(alloc(p, &d.tri_uv, 3 * T));
@@ -213,6 +228,7 @@ cudaError_t allocate_event(edp_peeler *p) {
     largest = v > largest ? v : largest;
   int64_t scan = R > E ? R : E;
   scan = S > scan ? S : scan;  // the segment-slot compaction
+  scan = std::max(scan, int64_t(d.grid_layers) * d.grid_size * d.grid_size);
   return allocate_scratch(p, largest, scan);
 }
 
@@ -244,7 +260,8 @@ cudaError_t allocate_device(edp_peeler *p) {
   for (int64_t v : {p->point_tree.leaves_cap, p->seg_tree.leaves_cap, p->source_tree.leaves_cap,
                     p->residual_tree.leaves_cap})
     largest = v > largest ? v : largest;
-  return allocate_scratch(p, largest, R > E ? R : E);
+  return allocate_scratch(p, largest,
+                         std::max({R, E, int64_t(d.grid_layers) * d.grid_size * d.grid_size}));
 }
 
 // Stage sequence of each peeler.  The loop body runs while the device sets
