@@ -211,11 +211,12 @@ __device__ inline int query_next(const Tree &t, int leaves, float4 lo, float4 hi
 // below the root so that every later group, leaf groups included, is 32 wide.
 // Groups are expanded depth first, lowest lane first, so leaf batches come out
 // in increasing leaf order: the candidates, and their order, are exactly those
-// of the binary successor walk above.  Only leaves at or after `cursor` are
+// of the binary successor walk above.  Only leaves in [cursor, end) are
 // produced.  Every member is warp-uniform; all 32 lanes must call together.
 struct WarpWalk {
   int levels;      // leaves = 2^levels
   int top;         // level of the first group
+  int end;         // first leaf past the walked range
   int depth, level, base, width;
   // Overlapping, not yet expanded nodes per depth (lane bits).  Leaves fit an
   // int, so there are at most 30 levels and depths 0..5; the depth is
@@ -250,14 +251,17 @@ __device__ inline unsigned walk_test(const Tree &t, int leaves, const WarpWalk &
   bool hit = false;
   if (lane < w.width) {
     const int node = w.base + lane;
-    const int last = ((node + 1) << (w.levels - w.level)) - leaves - 1;  // last leaf below
-    if (last >= cursor) hit = overlaps(__ldg(&t.nodes[2 * node]), __ldg(&t.nodes[2 * node + 1]), lo, hi);
+    const int first = (node << (w.levels - w.level)) - leaves;  // leaves below: [first, last]
+    const int last = ((node + 1) << (w.levels - w.level)) - leaves - 1;
+    if (last >= cursor && first < w.end)
+      hit = overlaps(__ldg(&t.nodes[2 * node]), __ldg(&t.nodes[2 * node + 1]), lo, hi);
   }
   return __ballot_sync(0xffffffffu, hit);
 }
 
 __device__ inline void walk_begin(WarpWalk &w, const Tree &t, int leaves, float4 lo, float4 hi,
-                                  int cursor) {
+                                  int cursor, int end = 0x7fffffff) {
+  w.end = end;
   w.levels = 31 - __clz(leaves);
   w.top = w.levels == 0 ? 0 : (w.levels - 1) % 5 + 1;
   w.depth = 0;
@@ -265,7 +269,7 @@ __device__ inline void walk_begin(WarpWalk &w, const Tree &t, int leaves, float4
   w.base = 1 << w.top;
   w.width = 1 << w.top;
   w.p1 = w.p2 = w.p3 = w.p4 = w.p5 = 0u;
-  w.p0 = cursor < leaves ? walk_test(t, leaves, w, lo, hi, cursor) : 0u;
+  w.p0 = cursor < leaves && cursor < end ? walk_test(t, leaves, w, lo, hi, cursor) : 0u;
 }
 
 // Advance to the next leaf batch: bit i of `batch` marks an overlapping leaf

@@ -481,15 +481,24 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
   const int leaves = *d.source_tree.size;
   const long long jobs = d.metrics[kHeavyRayGroups];
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  // Few rays share the GPU: split each one's rest into `parts` ranges of
+  // whole leaf groups, about 32K warp tasks in all (event_kernels.py:248-298).
+  int parts = 1;
+  while (parts * 2LL * jobs <= 32768 && parts * 2 * 32 <= leaves) parts *= 2;
+  const int width = leaves / parts;
   long long tests = 0;  // lane 0's tally
-  for (int64_t j = tid() >> 5; j < jobs; j += warps) {
-    const int2 job = d.heavy_queries[j];
-    const int i = job.x, cursor = job.y - leaves;  // job.y: the first leaf node left
+  for (int64_t task = tid() >> 5; task < jobs * parts; task += warps) {
+    const int2 job = d.heavy_queries[task / parts];
+    const int part = int(task % parts), end = (part + 1) * width;
+    const int i = job.x;
+    int cursor = job.y - leaves;  // job.y: the first leaf node left
+    if (cursor >= end) continue;
+    cursor = max(cursor, part * width);
     const V2 x = d.samples[i];
     const float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     const float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
     WarpWalk w;
-    walk_begin(w, d.source_tree, leaves, lo, hi, cursor);
+    walk_begin(w, d.source_tree, leaves, lo, hi, cursor, end);
     int budget = 0x7fffffff, first, resume, found = 0;
     unsigned batch;
     bool overflow = false;
