@@ -84,6 +84,8 @@ struct Caps {
   int64_t frontier, regions, hits, vertices, triangles, rounds, layers, edge_vertices;
 };
 
+constexpr int kRayCells = 16;  // most source-grid cells one source is listed in
+
 // Device scalars kept between kernels of one extraction.
 enum Scalar : int {
   kLivePolygons = 0,   // min(status[2], regions)
@@ -100,8 +102,12 @@ enum Scalar : int {
   kGridOn = 11,        // 1 when the point grid holds every layer of this extraction
   kGridCells = 12,     // grid cells in use: layers x G^2 when the grid is on, else 0
   kTreePoints = 13,    // points of the point hierarchy: 0 when the grid is on
+  kHeavyJobs = 14,     // rays queued for the continuation
+  kRayGridOn = 15,     // 1 when rays read their candidates from the source grid
+  kRayBig = 16,        // sources too large for the grid's cells
+  kRayGridCells = 17,  // G^2 (constant): cells of the source grid
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
-  kScalarCount = 16
+  kScalarCount = 24
 };
 
 // Every device pointer of a workspace, passed by value to the kernels.
@@ -187,6 +193,11 @@ struct Dev {
   // grid_layers layers; cell_start is the exclusive scan of the per-cell point
   // counts (with the total at the end) and grid_pts the points by cell.
   int grid_size, grid_layers;
+  // Source grid for rays (EventPeeler): the same G x G cells over the window,
+  // listing each source whose box (grown by 1e-6) meets at most kRayCells of
+  // them; larger sources in ray_big.  leaf_of: each source's leaf in the
+  // source hierarchy.
+  int *ray_count, *ray_start, *ray_entries, *ray_big, *leaf_of;
   int *cell_count, *cell_start;
   V2 *grid_pts;
   float4 *pt_lo, *pt_hi;

@@ -404,6 +404,67 @@ __device__ inline bool contains_flat(const Dev &d, int source, V2 x) {
   return n > 0;
 }
 
+// ---------------------------------------------------------------- source grid
+// Grid column (or row) of a window coordinate: floor(v G) clamped to the grid.
+__device__ inline int ray_cell(double v, int g) {
+  const double c = floor(v * double(g));
+  return c < 0.0 ? 0 : c > double(g - 1) ? g - 1 : int(c);
+}
+
+// Cells of a source's box grown by 1e-6 (a ray's query box, x +- 2e-7 in
+// binary32, meets the box only if the ray's point lies in this range); false
+// for an empty box.
+__device__ inline bool source_cells(const Dev &d, int s, int &cx0, int &cx1, int &cy0, int &cy1) {
+  const float4 lo = d.src_lo[s], hi = d.src_hi[s];
+  if (!(lo.x <= hi.x && lo.y <= hi.y)) return false;
+  const int g = d.grid_size;
+  cx0 = ray_cell(double(lo.x) - 1.0e-6, g);
+  cx1 = ray_cell(double(hi.x) + 1.0e-6, g);
+  cy0 = ray_cell(double(lo.y) - 1.0e-6, g);
+  cy1 = ray_cell(double(hi.y) + 1.0e-6, g);
+  return true;
+}
+
+__global__ void k_ray_grid_count(Dev d) {
+  if (tid() == 0) d.sc[kRayGridCells] = d.grid_size * d.grid_size;
+  for (int64_t s = tid(); s < d.n; s += stride()) {
+    int cx0, cx1, cy0, cy1;
+    if (!source_cells(d, int(s), cx0, cx1, cy0, cy1)) continue;
+    if ((cx1 - cx0 + 1) * (cy1 - cy0 + 1) > kRayCells) {
+      d.ray_big[reserve(&d.sc[kRayBig], 1)] = int(s);
+      continue;
+    }
+    for (int cy = cy0; cy <= cy1; ++cy)
+      for (int cx = cx0; cx <= cx1; ++cx) atomicAdd(&d.ray_count[cy * d.grid_size + cx], 1);
+  }
+}
+
+// Counting sort: ray_start is the scan of the counts; each listing takes a
+// slot of its cell.  The grid serves the rays when few sources are big.
+__global__ void k_ray_grid_fill(Dev d) {
+  if (tid() == 0) d.sc[kRayGridOn] = d.sc[kRayBig] <= 64 ? 1 : 0;
+  for (int64_t s = tid(); s < d.n; s += stride()) {
+    int cx0, cx1, cy0, cy1;
+    if (!source_cells(d, int(s), cx0, cx1, cy0, cy1)) continue;
+    if ((cx1 - cx0 + 1) * (cy1 - cy0 + 1) > kRayCells) continue;
+    for (int cy = cy0; cy <= cy1; ++cy)
+      for (int cx = cx0; cx <= cx1; ++cx) {
+        const int c = cy * d.grid_size + cx;
+        d.ray_entries[d.ray_start[c] + atomicSub(&d.ray_count[c], 1) - 1] = int(s);
+      }
+  }
+}
+
+// Each source's leaf in the source hierarchy (the order of its binary walk).
+__global__ void k_leaf_of(Dev d) {
+  const int count = d.n;
+  const int leaves = *d.source_tree.size;
+  for (int64_t leaf = tid(); leaf < leaves; leaf += stride()) {
+    const int s = d.source_tree.ids[leaf];
+    if (s < count) d.leaf_of[s] = int(leaf);
+  }
+}
+
 // Hits found by one thread, flushed to the shared pool with one reservation.
 struct HitBuffer {
   static constexpr int kSize = kCandidatesPerPass;
@@ -431,15 +492,43 @@ struct HitBuffer {
 __global__ void k_ray_hits(Dev d) {
   const int live = live_polygons(d);
   const int leaves = *d.source_tree.size;
-  long long groups = 0, tests = 0;
+  const bool grid = d.sc[kRayGridOn] != 0;
+  long long groups = 0, tests = 0, heavy_rays = 0;
   HitBuffer hits;
   for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
-    const int i = d.order[k];  // spatial order: neighbouring rays walk neighbouring nodes
+    const int i = d.order[k];  // spatial order: neighbouring rays read neighbouring data
     if (d.groups[i] != i) continue;
     V2 x = d.samples[i];
     float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), 1.0e30f, 0.f);
+    ++groups;
+    if (grid) {
+      // Every source whose box meets the query box is listed in the point's
+      // cell (or among the big ones); the box test keeps exactly the
+      // hierarchy's candidates, the whole ray in one pass.
+      const int g = d.grid_size, c = ray_cell(x.y, g) * g + ray_cell(x.x, g);
+      const int begin = d.ray_start[c], end = d.ray_start[c + 1], big = d.sc[kRayBig];
+      int met = 0, last = -1, found = 0;
+      for (int e = begin; e < end + big; ++e) {
+        const int s = e < end ? d.ray_entries[e] : d.ray_big[e - end];
+        if (!overlaps(d.src_lo[s], d.src_hi[s], lo, hi)) continue;
+        ++met;
+        last = max(last, d.leaf_of[s]);
+        if (contains_flat(d, s, x)) {
+          hits.source[hits.count] = s;
+          hits.depth[hits.count] = value(d.scores[s], x);
+          ++found;
+          if (++hits.count == HitBuffer::kSize) hits.flush(d, i);
+        }
+      }
+      if (hits.count) hits.flush(d, i);
+      d.group_counts[i] = found;
+      tests += met;
+      // The binary walk's primary pass would leave this ray unfinished.
+      heavy_rays += met > kCandidatesPerPass || (met == kCandidatesPerPass && last != leaves - 1);
+      continue;
+    }
     int node = 1;
     for (int step = 0; step < kCandidatesPerPass; ++step) {
       int s;
@@ -455,15 +544,16 @@ __global__ void k_ray_hits(Dev d) {
     }
     d.group_counts[i] = hits.count;
     hits.flush(d, i);
-    ++groups;
     const bool heavy = node > 0;
     if (heavy)
       while (node < leaves) node *= 2;
-    int slot = int(reserve(&d.metrics[kHeavyRayGroups], heavy ? 1 : 0));
+    heavy_rays += heavy;
+    int slot = reserve(&d.sc[kHeavyJobs], heavy ? 1 : 0);
     if (heavy) d.heavy_queries[slot] = make_int2(i, node);
   }
   count_add(&d.metrics[kRayGroups], groups);
   count_add(&d.metrics[kRayCandidateTests], tests);
+  count_add(&d.metrics[kHeavyRayGroups], heavy_rays);
 }
 
 // The continuation of the rays whose primary pass did not finish, one warp
@@ -479,7 +569,7 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int leaves = *d.source_tree.size;
-  const long long jobs = d.metrics[kHeavyRayGroups];
+  const long long jobs = d.sc[kHeavyJobs];
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   // Few rays share the GPU: split each one's rest into `parts` ranges of
   // whole leaf groups, about 32K warp tasks in all (event_kernels.py:248-298).
@@ -811,6 +901,18 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_certify_heavy<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
     note_launch();
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
+    note_launch();
+  }
+  {
+    const int64_t cells = int64_t(d.grid_size) * d.grid_size;
+    EDP_CHECK(cudaMemsetAsync(d.ray_count, 0, sizeof(int) * cells, st));
+    k_leaf_of<<<blocks(d.n), kBlock, 0, st>>>(d);
+    note_launch();
+    k_ray_grid_count<<<blocks(d.n), kBlock, 0, st>>>(d);
+    note_launch();
+    EDP_CHECK(scan_exclusive(d.ray_count, d.ray_start, d.sc + kRayGridCells, cells,
+                             d.ray_start + cells, s, st));
+    k_ray_grid_fill<<<blocks(d.n), kBlock, 0, st>>>(d);
     note_launch();
   }
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);

@@ -197,6 +197,14 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.cell_valid, 1024));
   EDP_CHECK(alloc(p, &d.heavy_beams, 1024));
   EDP_CHECK(alloc(p, &d.heavy_queries, R));
+  {
+    const int64_t cells = int64_t(d.grid_size) * d.grid_size;
+    EDP_CHECK(alloc(p, &d.ray_count, cells));
+    EDP_CHECK(alloc(p, &d.ray_start, cells + 1));
+    EDP_CHECK(alloc(p, &d.ray_entries, int64_t(kRayCells) * (n > 0 ? n : 1)));
+    EDP_CHECK(alloc(p, &d.ray_big, n > 0 ? n : 1));
+    EDP_CHECK(alloc(p, &d.leaf_of, n > 0 ? n : 1));
+  }
   EDP_CHECK(alloc(p, &d.group_counts, R));
   EDP_CHECK(alloc(p, &d.group_offsets, R));
   EDP_CHECK(alloc(p, &d.group_fill, R));
