@@ -85,6 +85,7 @@ struct Caps {
 };
 
 constexpr int kRayCells = 16;  // most source-grid cells one source is listed in
+constexpr int kSegCells = 4;   // most segment-grid cells one contour segment is listed in
 
 // Device scalars kept between kernels of one extraction.
 enum Scalar : int {
@@ -105,7 +106,9 @@ enum Scalar : int {
   kHeavyJobs = 14,     // rays queued for the continuation
   kRayGridOn = 15,     // 1 when rays read their candidates from the source grid
   kRayBig = 16,        // sources too large for the grid's cells
-  kRayGridCells = 17,  // G^2 (constant): cells of the source grid
+  kRayGridCells = 17,  // G^2 (constant): cells of the source and segment grids
+  kSegGridOn = 18,     // 1 when connection tests read segments from the segment grid
+  kSegBig = 19,        // contour segments too large for the grid's cells
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 24
 };
@@ -198,6 +201,9 @@ struct Dev {
   // them; larger sources in ray_big.  leaf_of: each source's leaf in the
   // source hierarchy.
   int *ray_count, *ray_start, *ray_entries, *ray_big, *leaf_of;
+  // Contour segment grid for the connection test: distinct segments listed in
+  // the cells their box (grown by 1e-6) meets, at most kSegCells each.
+  int *seg_count, *seg_start, *seg_entries, *seg_big;
   int *cell_count, *cell_start;
   V2 *grid_pts;
   float4 *pt_lo, *pt_hi;

@@ -19,6 +19,7 @@ __global__ void k_reset(Dev d) {
   if (i == 0) {
     d.sc[kSourceCount] = d.n;
     d.sc[kSegmentSlots] = kSourceVertices * d.n;
+    d.sc[kRayGridCells] = d.grid_size * d.grid_size;
     *d.parity = 0;
     *d.condition = 0;
   }

@@ -146,8 +146,60 @@ __device__ inline void uf_unite(int *parents, int a, int b) {
   }
 }
 
+// Contour-segment grid (the same cells as the source grid): each distinct
+// segment whose box, grown by 1e-6, meets at most kSegCells cells is listed
+// in them; longer ones go to a list every query reads.
+__device__ inline int seg_grid_cell(double v, int g) {
+  const double c = floor(v * double(g));
+  return c < 0.0 ? 0 : c > double(g - 1) ? g - 1 : int(c);
+}
+
+__device__ inline bool segment_cells(const Dev &d, int c, int &cx0, int &cx1, int &cy0, int &cy1) {
+  const float4 lo = d.seg_lo[c], hi = d.seg_hi[c];
+  if (!(lo.x <= hi.x && lo.y <= hi.y)) return false;
+  const int g = d.grid_size;
+  cx0 = seg_grid_cell(double(lo.x) - 1.0e-6, g);
+  cx1 = seg_grid_cell(double(hi.x) + 1.0e-6, g);
+  cy0 = seg_grid_cell(double(lo.y) - 1.0e-6, g);
+  cy1 = seg_grid_cell(double(hi.y) + 1.0e-6, g);
+  return true;
+}
+
+__global__ void k_seg_grid_count(Dev d) {
+  const int total = d.sc[kSegmentCount];
+  for (int64_t c = tid(); c < total; c += stride()) {
+    int cx0, cx1, cy0, cy1;
+    if (!segment_cells(d, int(c), cx0, cx1, cy0, cy1)) continue;
+    if ((cx1 - cx0 + 1) * (cy1 - cy0 + 1) > kSegCells) {
+      d.seg_big[reserve(&d.sc[kSegBig], 1)] = int(c);
+      continue;
+    }
+    for (int cy = cy0; cy <= cy1; ++cy)
+      for (int cx = cx0; cx <= cx1; ++cx) atomicAdd(&d.seg_count[cy * d.grid_size + cx], 1);
+  }
+}
+
+__global__ void k_seg_grid_fill(Dev d) {
+  if (tid() == 0) d.sc[kSegGridOn] = d.sc[kSegBig] <= 64 ? 1 : 0;
+  const int total = d.sc[kSegmentCount];
+  for (int64_t c = tid(); c < total; c += stride()) {
+    int cx0, cx1, cy0, cy1;
+    if (!segment_cells(d, int(c), cx0, cx1, cy0, cy1)) continue;
+    if ((cx1 - cx0 + 1) * (cy1 - cy0 + 1) > kSegCells) continue;
+    for (int cy = cy0; cy <= cy1; ++cy)
+      for (int cx = cx0; cx <= cx1; ++cx) {
+        const int cell = cy * d.grid_size + cx;
+        d.seg_entries[d.seg_start[cell] + atomicSub(&d.seg_count[cell], 1) - 1] = int(c);
+      }
+  }
+}
+
 // Matched edges are connected when no nearer-or-equal contour passes through
-// the edge midpoint (components.py:393-450).
+// the edge midpoint (components.py:393-450).  Candidate segments are those
+// whose box meets the query box: from the segment grid's cell of the midpoint
+// (every such segment is listed there or among the long ones), else from the
+// contour hierarchy.  Any blocking segment decides, so the order does not
+// matter; the visit counter counts segments met until the first blocker.
 __global__ void k_connect(Dev d) {
   const int total = d.sc[kPatchEdges];
   const int leaves = *d.seg_tree.size;
@@ -163,12 +215,10 @@ __global__ void k_connect(Dev d) {
     double pad = 2.0e-7 * fmax(1.0, fabs(z));
     float4 lo = make_float4(lower_f(x.x - 2.0e-7), lower_f(x.y - 2.0e-7), -1.0e30f, 0.f);
     float4 hi = make_float4(upper_f(x.x + 2.0e-7), upper_f(x.y + 2.0e-7), upper_f(z + pad), 0.f);
-    int node = 1, visits = 0;
+    int visits = 0;
     bool safe = true;
-    while (node > 0) {
-      int c;
-      node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
-      if (c < 0) break;
+    // Does segment c pass through x at or in front of the patch?
+    auto blocks = [&](int c) {
       ++visits;
       V2 u = d.seg_a[c], v = d.seg_b[c], dv = v - u;
       double len = length(dv);
@@ -177,10 +227,32 @@ __global__ void k_connect(Dev d) {
         if (fabs(cross(u, v, x)) <= kEps * len && t >= -kEps / len && t <= 1.0 + kEps / len) {
           V2 near = d.seg_near[c];
           double depth = near.x + t * (near.y - near.x);
-          if (depth <= z + pad) {
-            safe = false;
-            break;
-          }
+          if (depth <= z + pad) return true;
+        }
+      }
+      return false;
+    };
+    if (d.sc[kSegGridOn]) {
+      const int g = d.grid_size;
+      const int cell = seg_grid_cell(x.y, g) * g + seg_grid_cell(x.x, g);
+      const int begin = d.seg_start[cell], end = d.seg_start[cell + 1], big = d.sc[kSegBig];
+      for (int e = begin; e < end + big; ++e) {
+        const int c = e < end ? d.seg_entries[e] : d.seg_big[e - end];
+        if (!overlaps(d.seg_lo[c], d.seg_hi[c], lo, hi)) continue;
+        if (blocks(c)) {
+          safe = false;
+          break;
+        }
+      }
+    } else {
+      int node = 1;
+      while (node > 0) {
+        int c;
+        node = query_next(d.seg_tree, leaves, lo, hi, node, 0, c);
+        if (c < 0) break;
+        if (blocks(c)) {
+          safe = false;
+          break;
         }
       }
     }
@@ -426,7 +498,6 @@ __device__ inline bool source_cells(const Dev &d, int s, int &cx0, int &cx1, int
 }
 
 __global__ void k_ray_grid_count(Dev d) {
-  if (tid() == 0) d.sc[kRayGridCells] = d.grid_size * d.grid_size;
   for (int64_t s = tid(); s < d.n; s += stride()) {
     int cx0, cx1, cy0, cy1;
     if (!source_cells(d, int(s), cx0, cx1, cy0, cy1)) continue;
@@ -880,7 +951,17 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     EDP_CHECK(cudaMemsetAsync(d.edge_hash, 0xff, sizeof(int) * (int64_t(d.edge_hash_mask) + 1), st));
     k_match_edges<<<blocks(E), kBlock, 0, st>>>(d);
     note_launch();
-    if (d.propagate_ranks) k_connect<<<blocks(E), kBlock, 0, st>>>(d);
+    if (d.propagate_ranks) {
+      const int64_t cells = int64_t(d.grid_size) * d.grid_size;
+      EDP_CHECK(cudaMemsetAsync(d.seg_count, 0, sizeof(int) * cells, st));
+      k_seg_grid_count<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+      note_launch();
+      EDP_CHECK(scan_exclusive(d.seg_count, d.seg_start, d.sc + kRayGridCells, cells,
+                               d.seg_start + cells, s, st));
+      k_seg_grid_fill<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
+      note_launch();
+      k_connect<<<blocks(E), kBlock, 0, st>>>(d);
+    }
     note_launch();
   }
   k_roots<<<blocks(R), kBlock, 0, st>>>(d, d.propagate_ranks ? 1 : 0);

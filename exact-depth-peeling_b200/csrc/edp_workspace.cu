@@ -204,6 +204,10 @@ cudaError_t allocate_event(edp_peeler *p) {
     EDP_CHECK(alloc(p, &d.ray_entries, int64_t(kRayCells) * (n > 0 ? n : 1)));
     EDP_CHECK(alloc(p, &d.ray_big, n > 0 ? n : 1));
     EDP_CHECK(alloc(p, &d.leaf_of, n > 0 ? n : 1));
+    EDP_CHECK(alloc(p, &d.seg_count, cells));
+    EDP_CHECK(alloc(p, &d.seg_start, cells + 1));
+    EDP_CHECK(alloc(p, &d.seg_entries, int64_t(kSegCells) * S));
+    EDP_CHECK(alloc(p, &d.seg_big, S));
   }
   EDP_CHECK(alloc(p, &d.group_counts, R));
   EDP_CHECK(alloc(p, &d.group_offsets, R));
