@@ -122,9 +122,9 @@ __global__ void k_unique_points(Dev d) {
   }
 }
 
-// Sort key of each live output polygon: the 15-bit-per-axis Morton code of
-// its box centre (the key layout of the hierarchies, kernels.py:67-91), below
-// its layer when `layered`.
+// Sort key of each live output polygon: the Morton code of its box centre
+// (the 15-bit-per-axis code of the hierarchies, kernels.py:67-91, cut to 12
+// bits per axis), below its layer when `layered`.
 __global__ void k_order_keys(Dev d, int layered) {
   const int live = d.sc[kLivePolygons];
   for (int64_t i = tid(); i < live; i += stride()) {
@@ -138,8 +138,9 @@ __global__ void k_order_keys(Dev d, int layered) {
     const float cx = fminf(fmaxf(float(0.5 * (lx + hx)), 0.f), 1.f);
     const float cy = fminf(fmaxf(float(0.5 * (ly + hy)), 0.f), 1.f);
     const uint32_t x = uint32_t(int(cx * 32767.0f)), y = uint32_t(int(cy * 32767.0f));
-    uint64_t key = part1by1(x) | (part1by1(y) << 1);
-    if (layered) key |= uint64_t(uint32_t(d.out_layer[i]) & 0xffffu) << 32;
+    // 12 bits per axis (a 4096 x 4096 grid) are plenty for locality.
+    uint64_t key = (part1by1(x) | (part1by1(y) << 1)) >> 6;
+    if (layered) key |= uint64_t(uint32_t(d.out_layer[i]) & 0xffffu) << 24;
     d.order_keys[i] = key;
     d.order[i] = int(i);
   }
@@ -338,9 +339,9 @@ cudaError_t order_polygons(const Dev &d, bool layered, SortScratch &s, cudaStrea
   const int64_t R = d.cap.regions;
   k_order_keys<<<blocks(R), kBlock, 0, st>>>(d, layered ? 1 : 0);
   note_launch();
-  // Layers fit 16 bits (at most 65536) above the 30 Morton bits.
+  // 16 layer bits above 24 Morton bits.
   return sort_pairs_u64(d.order_keys, d.order_keys_tmp, d.order, d.order_tmp,
-                        d.sc + kLivePolygons, R, layered ? 48 : 30, s, st);
+                        d.sc + kLivePolygons, R, layered ? 40 : 24, s, st);
 }
 
 cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tree,
