@@ -18,7 +18,10 @@ constexpr int kMaxVertices = 32;      // polygon register width (kernels.py:10)
 constexpr int kSourceVertices = 8;    // triangle + near plane + 4 window planes
 constexpr double kEps = 1.0e-10;      // cleanup scale in the unit window (kernels.py:11)
 constexpr float kPad = 2.0e-7f;       // binary32 box padding (kernels.py:244-249)
-constexpr int kCandidatesPerPass = 32;  // bounded traversal per thread (frontier.py:149)
+// The reference's per-pass candidate bound (frontier.py:149,
+// event_kernels.py:196-245): the primary ray pass of the hierarchy path and
+// the definition of a heavy ray.
+constexpr int kCandidatesPerPass = 32;
 
 // Status slots (kernels.py:17-21, warp_peel/README.md:175-184).
 enum StatusSlot : int {

@@ -1,5 +1,6 @@
-// Mesh stage: boundary vertex gathering, the layered point hierarchy and
-// per-edge noding, centroid-fan triangulation and world lifting
+// Mesh stage: boundary vertex gathering and deduplication, the layered point
+// grid (or, for very deep scenes, the layered point hierarchy), per-polygon
+// noding, centroid-fan triangulation and world lifting
 // (warp_peel/kernels.py:941-1204, events.py:720-780).
 #include "edp_internal.h"
 

@@ -1,7 +1,9 @@
-// Rank stage: certified patch connectivity, canonical samples, shared query
-// groups with certified rectangles, ray hit gathering, the stable hit order
-// and per-polygon rank assignment (warp_peel/events.py:291-635,
-// components.py, beams.py, event_kernels.py:28-385).
+// Rank stage: certified patch connectivity (over the contour-segment grid),
+// canonical samples, shared query groups with certified rectangles, ray hit
+// gathering (over the source grid, or the source hierarchy with its
+// continuation), the per-group hit order, per-polygon rank assignment and the
+// optional convex merge (warp_peel/events.py:291-635, components.py, beams.py,
+// event_kernels.py:28-385).
 #include "edp_internal.h"
 
 namespace edp {
