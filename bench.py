@@ -117,6 +117,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value, world, device):
+    """The largest of every rank's `value` (a time), through the process
+    group (NCCL on GPUs, gloo on CPUs); `value` itself on one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_ms_per_mesh(max_total_ms, steps, world):
+    """Replicas: every rank peels `steps` meshes in the slowest rank's time."""
+    return max_total_ms / (steps * world)
+
+
 def hbm_peak():
     try:
         return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
@@ -235,10 +253,7 @@ def run_batched(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     total = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    t = torch.tensor([total], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total = float(t.item())
+    total = max_over_ranks(total, world, device)
     ms_per_step = total / args.steps
     infos = batch.read_status()
     triangles = sum(i["triangles"] for i in infos)
@@ -291,7 +306,8 @@ def run_batched(args, rank, world, local_rank):
                "kind": "port", "sample": "2 views and 2 meshes of the batch, one extraction "
                                          "each, mean per mesh; excludes import and projection"}
     line = {
-        "metric": METRIC, "value": ms_per_step / (meshes * world), "unit": UNIT,
+        "metric": METRIC, "value": whole_job_ms_per_mesh(total, args.steps * meshes, world),
+        "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -355,11 +371,8 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     total = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    launches_ms = torch.tensor([total], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(launches_ms, op=dist.ReduceOp.MAX)
-    total = float(launches_ms.item())
-    ms_per_mesh = total / (args.steps * world)
+    total = max_over_ranks(total, world, device)
+    ms_per_mesh = whole_job_ms_per_mesh(total, args.steps, world)
     check = p.read_status()
     # Stage timing, as the reference profiles (scripts/profile_events.py): each
     # stage replayed alone from its own captured graph, CUDA events on the
@@ -404,10 +417,7 @@ def run_ours(args, rank, world, local_rank):
                 buf[:got].copy_(getattr(p, name)[:got], non_blocking=True)
         stream.synchronize()
     e2e_ms = 1000.0 * (time.perf_counter() - t0) / max(e2e_steps, 1)
-    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(e2e_t.item()) / world
+    e2e_ms = max_over_ranks(e2e_ms, world, device) / world
     h2d = sum(a.numel() * a.element_size() for a in pinned)
     d2h_bytes = 64 + 152 + 128 * t_count
 
