@@ -384,33 +384,47 @@ __device__ inline void cell_box(const Dev &d, int c, float4 &lo, float4 &hi) {
 // every source candidate strictly covers the cell's sample rectangle; on
 // intersection-resolved input the covering set and its depth order are then
 // constant over the rectangle (beams.py:109-146).
-__global__ void k_certify(Dev d) {
-  const int c = int(tid());
+__global__ void __launch_bounds__(kBlock) k_certify(Dev d) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int c = int(tid() >> 5);  // one warp per cell
   if (c >= kCells || d.status[kError] != 0 || d.cell_min[c] == 0x7fffffff) return;
   const double *b = d.cell_bounds + 4 * c;
   if (b[0] == b[2] && b[1] == b[3]) return;  // identical samples already share
-  add_metric(d, kBeamAttempts, 1);
   float4 lo, hi;
   cell_box(d, c, lo, hi);
   const int leaves = *d.source_tree.size;
-  int node = 1, visits = 0, accepted = 1;
-  for (int step = 0; step < kCandidatesPerPass; ++step) {
-    int s;
-    node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
-    if (s < 0) break;
-    ++visits;
-    if (!covers(d, s, c)) {
+  // Up to kCandidatesPerPass candidates in leaf order, a candidate per lane;
+  // the first one that does not cover the cell rejects it.
+  WarpWalk w;
+  walk_begin(w, d.source_tree, leaves, lo, hi, 0);
+  int budget = 0x7fffffff, first, resume, met = 0, accepted = 1, last = -1;
+  unsigned batch;
+  while (met < kCandidatesPerPass &&
+         walk_next(w, d.source_tree, leaves, lo, hi, 0, budget, batch, first, resume)) {
+    unsigned take = batch;
+    for (int extra = __popc(take) - (kCandidatesPerPass - met); extra > 0; --extra)
+      take &= ~(1u << (31 - __clz(take)));  // drop the highest leaves past the budget
+    const bool bad = ((take >> lane) & 1u) && !covers(d, __ldg(&d.source_tree.ids[first + lane]), c);
+    const unsigned bads = __ballot_sync(full, bad);
+    if (bads) {
+      const int k = __ffs(int(bads)) - 1;
+      met += __popc(take & (full >> (31 - k)));  // met up to the rejecting one
       accepted = 0;
       break;
     }
-    if (node == 0) break;
+    met += __popc(take);
+    last = first + 31 - __clz(take);
   }
-  add_metric(d, kBeamCandidateTests, visits);
+  if (lane != 0) return;
+  add_metric(d, kBeamAttempts, 1);
+  add_metric(d, kBeamCandidateTests, met);
   d.cell_valid[c] = accepted;
-  if (accepted && node > 0) {
-    while (node < leaves) node *= 2;
+  // The binary walk would stop after its 32nd candidate with the rest of the
+  // hierarchy still to walk unless that candidate was the last leaf.
+  if (accepted && met == kCandidatesPerPass && last != leaves - 1) {
     int slot = int(atomicAdd(reinterpret_cast<unsigned long long *>(&d.metrics[kHeavyBeams]), 1ull));
-    d.heavy_beams[slot] = make_int2(c, node);
+    d.heavy_beams[slot] = make_int2(c, leaves + last + 1);
   }
 }
 
@@ -979,7 +993,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   k_group_resolve<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   if (d.share_regions) {
-    k_certify<<<kCells / 128, 128, 0, st>>>(d);
+    k_certify<<<kCells * 32 / kBlock, kBlock, 0, st>>>(d);
     note_launch();
     k_certify_heavy<<<kHeavyBlocks, kHeavyBlock, 0, st>>>(d);
     note_launch();
