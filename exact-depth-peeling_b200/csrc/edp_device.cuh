@@ -40,7 +40,8 @@ enum Metric : int {
   kTargetVisits = 0, kContourTests, kSplits, kRayGroups, kRayCandidateTests, kRayHits,
   kRounds, kUniqueContours, kHeavyRayGroups, kBeamAttempts, kCertifiedBeams,
   kBeamCandidateTests, kHeavyBeams, kRankComponents, kRankConnections,
-  kConnectionContourTests, kMergedPolygons, kMatchedPatchEdges, kEdgeHashMisses, kMetrics
+  kConnectionContourTests, kMergedPolygons, kMatchedPatchEdges, kEdgeHashMisses,
+  kHeavyNodedPolygons, kMetrics
 };
 
 // ---------------------------------------------------------------- vectors

@@ -109,6 +109,7 @@ enum Scalar : int {
   kRayGridCells = 17,  // G^2 (constant): cells of the source and segment grids
   kSegGridOn = 18,     // 1 when connection tests read segments from the segment grid
   kSegBig = 19,        // contour segments too large for the grid's cells
+  kHeavyPolygons = 20, // polygons queued for warp-wide noding
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
   kScalarCount = 24
 };
@@ -192,12 +193,14 @@ struct Dev {
   V2 *uverts;      // distinct (layer, point) vertices, indexed by the point hierarchy
   int *point_table;
   int point_mask;
-  // Layered point grid: G x G cells per layer over the unit window for up to
-  // grid_layers layers; cell_start is the exclusive scan of the per-cell point
-  // counts (with the total at the end) and grid_pts the points by cell.
-  int grid_size, grid_layers;
-  // Source grid for rays (EventPeeler): the same G x G cells over the window,
-  // listing each source whose box (grown by 1e-6) meets at most kRayCells of
+  // Layered point grid: point_grid x point_grid cells per layer over the
+  // unit window for up to grid_layers layers; cell_start is the exclusive scan
+  // of the per-cell point counts (with the total at the end) and grid_pts the
+  // points by cell.
+  int point_grid, grid_layers;
+  int grid_size;  // cells per axis of the source and segment grids
+  // Source grid for rays (EventPeeler): grid_size x grid_size cells over the
+  // window, listing each source whose box (grown by 1e-6) meets at most kRayCells of
   // them; larger sources in ray_big.  leaf_of: each source's leaf in the
   // source hierarchy.
   int *ray_count, *ray_start, *ray_entries, *ray_big, *leaf_of;
@@ -206,6 +209,7 @@ struct Dev {
   int *seg_count, *seg_start, *seg_entries, *seg_big;
   int *cell_count, *cell_start;
   V2 *grid_pts;
+  int *heavy_polygons;  // polygons with many grid candidates, noded a warp each
   float4 *pt_lo, *pt_hi;
   // A processing order of the live output polygons by the Morton code of
   // their box centre (optionally below the layer), rebuilt by each stage that

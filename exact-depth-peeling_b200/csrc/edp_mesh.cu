@@ -63,7 +63,13 @@ __global__ void k_grid_begin(Dev d) {
   const int layers = d.status[kLayers];
   const bool on = d.status[kError] == 0 && layers <= d.grid_layers;
   d.sc[kGridOn] = on ? 1 : 0;
-  d.sc[kGridCells] = on ? int(int64_t(layers) * d.grid_size * d.grid_size) : 0;
+  d.sc[kGridCells] = on ? int(int64_t(layers) * d.point_grid * d.point_grid) : 0;
+}
+
+// Zero the point counts of the cells this extraction uses.
+__global__ void k_grid_clear(Dev d) {
+  const int cells = d.sc[kGridCells];
+  for (int64_t c = tid(); c < cells; c += stride()) d.cell_count[c] = 0;
 }
 
 __global__ void k_tree_points(Dev d) {
@@ -74,7 +80,7 @@ __global__ void k_tree_points(Dev d) {
 // counts gives each cell's start, and each point takes a slot of its cell.
 __global__ void k_grid_scatter(Dev d) {
   if (!d.sc[kGridOn] || d.status[kError] != 0) return;
-  const int total = d.sc[kUniqueVertices], g = d.grid_size;
+  const int total = d.sc[kUniqueVertices], g = d.point_grid;
   if (tid() == 0) d.cell_start[d.sc[kGridCells]] = total;
   for (int64_t u = tid(); u < total; u += stride()) {
     const V2 x = d.uverts[u];
@@ -110,7 +116,7 @@ __global__ void k_unique_points(Dev d) {
     }
     const int u = reserve(&d.sc[kUniqueVertices], fresh ? 1 : 0);
     if (fresh && d.sc[kGridOn]) {
-      const int g = d.grid_size;
+      const int g = d.point_grid;
       atomicAdd(&d.cell_count[(int64_t(layer) * g + grid_cell(x.y, g)) * g + grid_cell(x.x, g)], 1);
     }
     if (fresh) {
@@ -168,6 +174,81 @@ __device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
 // box contains every edge's box) replaces the reference's query per edge; the
 // acceptance test and therefore the triangles are the same.
 constexpr int kPolygonSplits = 256;  // split points buffered per polygon
+// Candidate points x edges above which a polygon is noded by a whole warp
+// (k_mesh_heavy) rather than by one thread, so that a few large polygons in
+// dense cells do not hold 31 idle lanes of a warp.
+constexpr int kHeavyNodingWork = 1024;
+
+// The centroid fan of polygon p (n vertices, centroid `center`) through its
+// split points sorted by (edge, parameter).  Counts the fan triangles (signed
+// doubled area above EPS^2: noded points 1e-13 apart can otherwise give
+// slivers of area ~1e-19 whose orientation rounding decides; the reference
+// tests |area|, kernels.py:1105), reserves their slots at once, then writes
+// them with their world positions.
+__device__ inline void emit_fan(const Dev &d, const V2 *p, int n, V2 center, int layer,
+                                int source, const double *split_t,
+                                const unsigned char *split_edge, int count) {
+  int emitted = 0;
+  for (int e = 0, k = 0; e < n; ++e) {
+    const V2 a = p[e], dir = p[(e + 1) % n] - a;
+    double previous = 0.0;
+    V2 cursor = a;
+    for (;;) {
+      const bool last = !(k < count && split_edge[k] == e);
+      const double following = last ? 1.0 : split_t[k++];
+      if (following > previous + kEps) {
+        const V2 next = a + following * dir;
+        if (cross(center, cursor, next) > kEps * kEps) ++emitted;
+        cursor = next;
+        previous = following;
+      }
+      if (last) break;
+    }
+  }
+  int slot = reserve(&d.status[kTriangles], emitted);
+  if (int64_t(slot) + emitted > d.cap.triangles) {
+    set_error(d.status, kErrTriangles);
+    return;
+  }
+  const Plane sc = d.scores[source];
+  double w_center[3];
+  lift(d, center, sc, w_center);
+  for (int e = 0, k = 0; e < n; ++e) {
+    const V2 a = p[e], dir = p[(e + 1) % n] - a;
+    double previous = 0.0;
+    V2 cursor = a;
+    double w_cursor[3];
+    lift(d, cursor, sc, w_cursor);
+    for (;;) {
+      const bool last = !(k < count && split_edge[k] == e);
+      const double following = last ? 1.0 : split_t[k++];
+      if (following > previous + kEps) {
+        const V2 next = a + following * dir;
+        double w_next[3];
+        lift(d, next, sc, w_next);
+        if (cross(center, cursor, next) > kEps * kEps) {
+          V2 *uv = d.tri_uv + 3 * int64_t(slot);
+          double *w = d.tri_world + 9 * int64_t(slot);
+          uv[0] = center;
+          uv[1] = cursor;
+          uv[2] = next;
+          for (int c = 0; c < 3; ++c) {
+            w[c] = w_center[c];
+            w[3 + c] = w_cursor[c];
+            w[6 + c] = w_next[c];
+          }
+          d.tri_src[slot] = source;
+          d.tri_layer[slot] = layer;
+          ++slot;
+        }
+        cursor = next;
+        for (int c = 0; c < 3; ++c) w_cursor[c] = w_next[c];
+        previous = following;
+      }
+      if (last) break;
+    }
+  }
+}
 
 __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_capacity) {
   const int live = d.sc[kLivePolygons];
@@ -192,6 +273,24 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
                                   float(layer), 0.f);
     const float4 hi = make_float4(__double2float_ru(hx + 2.0e-7), __double2float_ru(hy + 2.0e-7),
                                   float(layer), 0.f);
+    // The grid cells meeting the polygon's box grown by 1e-9 hold every
+    // same-layer point within 1e-10 of its boundary, hence every split point.
+    const bool grid = d.sc[kGridOn] != 0;
+    const int g = d.point_grid;
+    const double qlx = lx - 1.0e-9, qly = ly - 1.0e-9, qhx = hx + 1.0e-9, qhy = hy + 1.0e-9;
+    const int cx0 = grid_cell(qlx, g), cx1 = grid_cell(qhx, g);
+    const int cy0 = grid_cell(qly, g), cy1 = grid_cell(qhy, g);
+    if (grid) {
+      int64_t candidates = 0;
+      for (int cy = cy0; cy <= cy1; ++cy) {
+        const int64_t row = (int64_t(layer) * g + cy) * g;
+        candidates += d.cell_start[row + cx1 + 1] - d.cell_start[row + cx0];
+      }
+      if (candidates * n > kHeavyNodingWork) {
+        d.heavy_polygons[atomicAdd(&d.sc[kHeavyPolygons], 1)] = int(i);
+        continue;
+      }
+    }
     int count = 0, per_edge[kMaxVertices];
     for (int e = 0; e < n; ++e) per_edge[e] = 0;
     bool overflow = false;
@@ -221,13 +320,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
         }
       }
     };
-    if (d.sc[kGridOn]) {
-      // The grid cells meeting the polygon's box grown by 1e-9 hold every
-      // same-layer point within 1e-10 of its boundary, hence every split point.
-      const int g = d.grid_size;
-      const double qlx = lx - 1.0e-9, qly = ly - 1.0e-9, qhx = hx + 1.0e-9, qhy = hy + 1.0e-9;
-      const int cx0 = grid_cell(qlx, g), cx1 = grid_cell(qhx, g);
-      for (int cy = grid_cell(qly, g); cy <= grid_cell(qhy, g) && !overflow; ++cy) {
+    if (grid) {
+      for (int cy = cy0; cy <= cy1 && !overflow; ++cy) {
         const int64_t row = (int64_t(layer) * g + cy) * g;
         const int end = d.cell_start[row + cx1 + 1];
         for (int j = d.cell_start[row + cx0]; j < end && !overflow; ++j) {
@@ -262,18 +356,142 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
       split_t[m + 1] = t;
       split_edge[m + 1] = e;
     }
-    // Count the fan triangles (signed doubled area above EPS^2: noded points
-    // 1e-13 apart can otherwise give slivers of area ~1e-19 whose orientation
-    // rounding decides; the reference tests |area|, kernels.py:1105), reserve
-    // their slots at once, then emit.
+    emit_fan(d, p, n, center, layer, source, split_t, split_edge, count);
+  }
+}
+
+// One polygon edge as the split-point test of k_mesh_polygons uses it, with
+// the quantities that test derives from the edge computed once.
+struct NodeEdge {
+  V2 a, b, dir;
+  double length2, slack, tol;
+};
+
+constexpr int kHeavyWarps = kBlock / 32;
+
+// Noding and emission of the polygons k_mesh_polygons queued as heavy, one
+// polygon per warp.  Lanes take the polygon's grid candidates 32 at a time
+// and test each against every edge with the thread kernel's expressions, so
+// the split points are the same.  Each split point is placed by its edge and
+// its rank along the edge, and the fan is written with a lane per edge.
+__global__ void __launch_bounds__(kBlock, 5) k_mesh_heavy(Dev d, int edge_capacity) {
+  __shared__ NodeEdge s_edge[kHeavyWarps][kMaxVertices];
+  __shared__ double s_t[kHeavyWarps][kPolygonSplits], s_sorted_t[kHeavyWarps][kPolygonSplits];
+  __shared__ unsigned char s_e[kHeavyWarps][kPolygonSplits];
+  __shared__ int s_count[kHeavyWarps], s_per_edge[kHeavyWarps][kMaxVertices];
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int heavy = d.sc[kHeavyPolygons];
+  if (tid() == 0) d.metrics[kHeavyNodedPolygons] = heavy;
+  const int g = d.point_grid;
+  NodeEdge *edges = s_edge[warp];
+  int *per_edge = s_per_edge[warp];
+  double *split_t = s_t[warp], *sorted_t = s_sorted_t[warp];
+  unsigned char *split_edge = s_e[warp];
+  for (int64_t h = tid() >> 5; h < heavy; h += stride() >> 5) {
+    int failed = 0;
+    if (lane == 0) failed = *(volatile int *)&d.status[kError];
+    if (__shfl_sync(kFull, failed, 0) != 0) return;
+    const int i = d.heavy_polygons[h];
+    const V2 *p = d.out_v + int64_t(kMaxVertices) * i;
+    const int n = d.out_n[i];
+    const int layer = d.out_layer[i], source = d.out_src[i];
+    // Box and centroid in the thread kernel's order (every lane alike).
+    double lx = 1.0e30, ly = 1.0e30, hx = -1.0e30, hy = -1.0e30;
+    V2 center = v2(0.0, 0.0);
+    for (int j = 0; j < n; ++j) {
+      const V2 x = p[j];
+      lx = fmin(lx, x.x); ly = fmin(ly, x.y);
+      hx = fmax(hx, x.x); hy = fmax(hy, x.y);
+      center = center + x / double(n);
+    }
+    if (lane < n) {
+      NodeEdge e;
+      e.a = p[lane];
+      e.b = p[(lane + 1) % n];
+      e.dir = e.b - e.a;
+      e.length2 = dot(e.dir, e.dir);
+      e.slack = 4.0 * kEps * kEps * e.length2;
+      e.tol = kEps * sqrt(e.length2);
+      edges[lane] = e;
+      per_edge[lane] = 0;
+    }
+    if (lane == 0) s_count[warp] = 0;
+    __syncwarp();
+    const double qlx = lx - 1.0e-9, qly = ly - 1.0e-9, qhx = hx + 1.0e-9, qhy = hy + 1.0e-9;
+    const int cx0 = grid_cell(qlx, g), cx1 = grid_cell(qhx, g);
+    const int cy0 = grid_cell(qly, g), cy1 = grid_cell(qhy, g);
+    for (int cy = cy0; cy <= cy1; ++cy) {
+      const int64_t row = (int64_t(layer) * g + cy) * g;
+      const int begin = d.cell_start[row + cx0], end = d.cell_start[row + cx1 + 1];
+      for (int j = begin + lane; j < end; j += 32) {
+        const V2 x = d.grid_pts[j];
+        if (x.x < qlx || x.x > qhx || x.y < qly || x.y > qhy) continue;
+        for (int e = 0; e < n; ++e) {
+          const NodeEdge &E = edges[e];
+          if (x == E.a || x == E.b) continue;
+          if (!(E.length2 > 0.0)) continue;
+          const double off = cross(E.a, E.b, x);
+          if (off * off > E.slack) continue;
+          const double tt = dot(x - E.a, E.dir) / E.length2;
+          if (tt > kEps && tt < 1.0 - kEps && fabs(off) <= E.tol) {
+            const int at = atomicAdd(&s_count[warp], 1);
+            atomicAdd(&per_edge[e], 1);
+            if (at < kPolygonSplits) {
+              split_t[at] = tt;
+              split_edge[at] = (unsigned char)e;
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // The thread kernel's overflow rule on the totals: more split points
+    // than the buffer, or more on one edge than edge_capacity.
+    const int count = s_count[warp];
+    if (__any_sync(kFull, lane < n && per_edge[lane] > edge_capacity) || count > kPolygonSplits) {
+      if (lane == 0) set_error(d.status, kErrEdgeNoding);
+      return;
+    }
+    // Edge e's split points take places [first_e, first_e + count_e) of the
+    // order by (edge, parameter): an exclusive scan of the per-edge counts.
+    const int mine = lane < n ? per_edge[lane] : 0;
+    int first = mine;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(kFull, first, off);
+      if (lane >= off) first += y;
+    }
+    first -= mine;
+    __syncwarp();
+    if (lane < n) per_edge[lane] = first;
+    __syncwarp();
+    // A split point's place: its edge's first place plus its rank among the
+    // edge's points by parameter, ties by arrival (equal parameters give the
+    // same triangles in either order).
+    for (int k = lane; k < count; k += 32) {
+      const double t = split_t[k];
+      const int e = split_edge[k];
+      int rank = per_edge[e];
+      for (int m = 0; m < count; ++m) {
+        const double tm = split_t[m];
+        rank += (split_edge[m] == e && (tm < t || (tm == t && m < k))) ? 1 : 0;
+      }
+      sorted_t[rank] = t;
+    }
+    __syncwarp();
+    // The fan of emit_fan() with a lane per edge: lane e walks its edge's
+    // split points, and the lanes' triangle counts are scanned in edge order,
+    // so the triangles and their order within the polygon are emit_fan()'s.
+    V2 a = v2(0.0, 0.0), dir = a;
     int emitted = 0;
-    for (int e = 0, k = 0; e < n; ++e) {
-      const V2 a = p[e], dir = p[(e + 1) % n] - a;
+    if (lane < n) {
+      a = edges[lane].a;
+      dir = edges[lane].dir;
       double previous = 0.0;
       V2 cursor = a;
-      for (;;) {
-        const bool last = !(k < count && split_edge[k] == e);
-        const double following = last ? 1.0 : split_t[k++];
+      for (int k = first;;) {
+        const bool last = k == first + mine;
+        const double following = last ? 1.0 : sorted_t[k++];
         if (following > previous + kEps) {
           const V2 next = a + following * dir;
           if (cross(center, cursor, next) > kEps * kEps) ++emitted;
@@ -283,23 +501,33 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
         if (last) break;
       }
     }
-    int slot = reserve(&d.status[kTriangles], emitted);
-    if (int64_t(slot) + emitted > d.cap.triangles) {
-      set_error(d.status, kErrTriangles);
+    int offset = emitted;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(kFull, offset, off);
+      if (lane >= off) offset += y;
+    }
+    const int total = __shfl_sync(kFull, offset, 31);
+    offset -= emitted;
+    int base = 0;
+    if (lane == 0 && total) base = atomicAdd(&d.status[kTriangles], total);
+    base = __shfl_sync(kFull, base, 0);
+    if (int64_t(base) + total > d.cap.triangles) {
+      if (lane == 0) set_error(d.status, kErrTriangles);
+      __syncwarp();
       continue;
     }
-    const Plane sc = d.scores[source];
-    double w_center[3];
-    lift(d, center, sc, w_center);
-    for (int e = 0, k = 0; e < n; ++e) {
-      const V2 a = p[e], dir = p[(e + 1) % n] - a;
+    if (lane < n) {
+      const Plane sc = d.scores[source];
+      double w_center[3];
+      lift(d, center, sc, w_center);
+      int slot = base + offset;
       double previous = 0.0;
       V2 cursor = a;
       double w_cursor[3];
       lift(d, cursor, sc, w_cursor);
-      for (;;) {
-        const bool last = !(k < count && split_edge[k] == e);
-        const double following = last ? 1.0 : split_t[k++];
+      for (int k = first;;) {
+        const bool last = k == first + mine;
+        const double following = last ? 1.0 : sorted_t[k++];
         if (following > previous + kEps) {
           const V2 next = a + following * dir;
           double w_next[3];
@@ -326,9 +554,9 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
         if (last) break;
       }
     }
+    __syncwarp();
   }
 }
-
 unsigned blocks(int64_t n) {
   int64_t g = ceil_div(n > 0 ? n : 1, kBlock);
   return unsigned(g < 148 * 16 ? g : 148 * 16);
@@ -355,9 +583,10 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   k_mesh_check<<<1, 1, 0, st>>>(d);
   note_launch();
   EDP_CHECK(cudaMemsetAsync(d.point_table, 0xff, sizeof(int) * (int64_t(d.point_mask) + 1), st));
-  const int64_t cells = int64_t(d.grid_layers) * d.grid_size * d.grid_size;
-  EDP_CHECK(cudaMemsetAsync(d.cell_count, 0, sizeof(int) * cells, st));
+  const int64_t cells = int64_t(d.grid_layers) * d.point_grid * d.point_grid;
   k_grid_begin<<<1, 1, 0, st>>>(d);
+  note_launch();
+  k_grid_clear<<<blocks(cells), kBlock, 0, st>>>(d);
   note_launch();
   k_scatter<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
@@ -374,7 +603,10 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
 
 cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st) {
   int cap = int(d.cap.edge_vertices < kMaxEdgeVertices ? d.cap.edge_vertices : kMaxEdgeVertices);
+  EDP_CHECK(cudaMemsetAsync(d.sc + kHeavyPolygons, 0, sizeof(int), st));
   k_mesh_polygons<<<blocks(d.cap.regions), kBlock, 0, st>>>(d, cap);
+  note_launch();
+  k_mesh_heavy<<<148 * 5, kBlock, 0, st>>>(d, cap);
   note_launch();
   return cudaGetLastError();
 }

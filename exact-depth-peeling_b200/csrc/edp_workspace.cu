@@ -124,17 +124,26 @@ cudaError_t allocate_shared(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.uverts, E));
   d.point_mask = table_mask(E);
   EDP_CHECK(alloc(p, &d.point_table, int64_t(d.point_mask) + 1));
-  // About sqrt(N) / 1.5 cells per axis (a power of two in [32, 512]), rows for
-  // as many layers as 16M cells allow.
+  // Source and segment grids: about sqrt(N) / 1.5 cells per axis (a power of
+  // two in [32, 512]).  Layered point grid: about 2 sqrt(N) cells per axis (a
+  // power of two in [32, 1024]; a front layer holds ~14 distinct boundary
+  // points per face, so its cells hold a few each), rows for as many layers as
+  // 256 N cells allow, at least 16M and at most 64M cells.
   {
     int g = 32;
     while (g < 512 && double(2 * g) * 1.5 <= std::sqrt(double(n > 0 ? n : 1))) g *= 2;
     d.grid_size = g;
-    const int64_t per_layer = int64_t(g) * g, budget = int64_t(1) << 24;
+    g = 32;
+    while (g < 1024 && double(2 * g) <= 2.0 * std::sqrt(double(n > 0 ? n : 1))) g *= 2;
+    d.point_grid = g;
+    const int64_t per_layer = int64_t(g) * g;
+    const int64_t budget =
+        std::max(int64_t(1) << 24, std::min(int64_t(1) << 26, int64_t(256) * (n > 0 ? n : 1)));
     d.grid_layers = int(std::min<int64_t>(d.cap.layers, std::max<int64_t>(1, budget / per_layer)));
     EDP_CHECK(alloc(p, &d.cell_count, d.grid_layers * per_layer));
     EDP_CHECK(alloc(p, &d.cell_start, d.grid_layers * per_layer + 1));
     EDP_CHECK(alloc(p, &d.grid_pts, E));
+    EDP_CHECK(alloc(p, &d.heavy_polygons, R));
   }
   EDP_CHECK(alloc(p, &d.pt_lo, E));
   EDP_CHECK(alloc(p, &d.pt_hi, E));
@@ -240,7 +249,7 @@ cudaError_t allocate_event(edp_peeler *p) {
     largest = v > largest ? v : largest;
   int64_t scan = R > E ? R : E;
   scan = S > scan ? S : scan;  // the segment-slot compaction
-  scan = std::max(scan, int64_t(d.grid_layers) * d.grid_size * d.grid_size);
+  scan = std::max(scan, int64_t(d.grid_layers) * d.point_grid * d.point_grid);
   return allocate_scratch(p, largest, scan);
 }
 
@@ -273,7 +282,7 @@ cudaError_t allocate_device(edp_peeler *p) {
                     p->residual_tree.leaves_cap})
     largest = v > largest ? v : largest;
   return allocate_scratch(p, largest,
-                         std::max({R, E, int64_t(d.grid_layers) * d.grid_size * d.grid_size}));
+                         std::max({R, E, int64_t(d.grid_layers) * d.point_grid * d.point_grid}));
 }
 
 // Stage sequence of each peeler.  The loop body runs while the device sets

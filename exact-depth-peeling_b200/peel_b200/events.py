@@ -13,7 +13,7 @@ import ctypes
 from dataclasses import dataclass
 
 from . import _lib
-from .solver import _Peeler, _Workspace, _check_inputs, _decode_status
+from .solver import METRIC_COUNT, _Peeler, _Workspace, _check_inputs, _decode_status
 
 
 @dataclass(frozen=True)
@@ -39,8 +39,9 @@ METRIC_NAMES = (
     "ray_hits", "rounds", "unique_contours", "heavy_ray_groups", "beam_attempts",
     "certified_beams", "beam_candidate_tests", "heavy_beams", "rank_components",
     "rank_connections", "connection_contour_tests", "merged_polygons", "matched_patch_edges",
-    "edge_hash_misses",
+    "edge_hash_misses", "heavy_noded_polygons",
 )
+assert len(METRIC_NAMES) == METRIC_COUNT
 
 
 class EventPeeler(_Peeler):

@@ -12,6 +12,8 @@ import numpy as np
 
 from . import _lib
 
+METRIC_COUNT = 20  # EDP_METRICS: workspace counters (include/edp.h)
+
 _ERROR_LABELS = {
     1: "polygon vertices",
     2: "per-worker pieces",
@@ -153,7 +155,7 @@ class _Workspace:
         R, T = int(o.regions), int(o.triangles)
         i32, f64 = (torch.int32, "<i4"), (torch.float64, "<f8")
         peeler.status = self.view(o.status, (16,), *i32)
-        peeler.metrics = self.view(o.metrics, (19,), torch.int64, "<i8")
+        peeler.metrics = self.view(o.metrics, (METRIC_COUNT,), torch.int64, "<i8")
         peeler.output = PolygonArray(self.view(o.output_vertices, (R, 32, 2), *f64),
                                      self.view(o.output_sizes, (R,), *i32))
         peeler.output_sources = self.view(o.output_sources, (R,), *i32)
@@ -172,7 +174,7 @@ class _Workspace:
 
     def read(self):
         status = np.zeros(16, dtype=np.int32)
-        metrics = np.zeros(19, dtype=np.int64)
+        metrics = np.zeros(METRIC_COUNT, dtype=np.int64)
         _lib.check(
             _lib.load().edp_read_status(self.handle, status.ctypes.data, metrics.ctypes.data),
             "read_status")

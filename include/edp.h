@@ -17,7 +17,7 @@
  *   edp_capture        warp_peel/solver.py:471-480  DevicePeeler.capture
  *   edp_run            warp_peel/solver.py:482-486  DevicePeeler.run
  *   edp_read_status    warp_peel/events.py:808-845  EventPeeler.read_status
- *                      (status[16] and metrics[19] arrays; solver.py:154-156,
+ *                      (status[16] and metrics[20] arrays; solver.py:154-156,
  *                      events.py:103)
  *   edp_get_outputs    the device attributes read by warp_peel/io.py:51-72
  *                      and tests/gpu/test_peeler.py:24-34
@@ -45,7 +45,7 @@ enum edp_status {
 /* Status slots and error bits (warp_peel/kernels.py:17-21, README.md:175-184). */
 enum {
   EDP_STATUS_SLOTS = 16,
-  EDP_METRICS = 19,
+  EDP_METRICS = 20,
   EDP_ERR_BIT_POLYGON = 1,
   EDP_ERR_BIT_WORKER = 2,
   EDP_ERR_BIT_RESIDUAL = 4,
@@ -80,7 +80,7 @@ typedef struct edp_device_capacities {
  * status[2] polygons, status[3] triangles, status[6] boundary vertices. */
 typedef struct edp_outputs {
   int32_t *status;          /* [16] */
-  int64_t *metrics;         /* [19] */
+  int64_t *metrics;         /* [20] */
   double *output_vertices;  /* [regions][32][2] polygon vertices */
   int32_t *output_sizes;    /* [regions] vertex counts (0 = suppressed) */
   int32_t *output_sources;  /* [regions] dense source (face) index */
@@ -122,7 +122,7 @@ int edp_enqueue(edp_peeler *p, void *stream);
 int edp_capture(edp_peeler *p);
 /* Asynchronous replay of the captured graph on the workspace stream. */
 int edp_run(edp_peeler *p);
-/* Synchronise the workspace stream and copy status[16] / metrics[19] out
+/* Synchronise the workspace stream and copy status[16] / metrics[20] out
  * (either may be NULL). */
 int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics);
 int edp_get_outputs(edp_peeler *p, edp_outputs *out);
