@@ -637,6 +637,6 @@ int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round) 
 
 int edp_last_cuda_error(void) { return g_last_cuda; }
 const char *edp_last_error_site(void) { return g_last_site; }
-int edp_abi_version(void) { return 1; }
+int edp_abi_version(void) { return EDP_ABI_VERSION; }
 
 }  // extern "C"

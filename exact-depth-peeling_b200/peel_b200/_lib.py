@@ -8,6 +8,7 @@ import ctypes
 from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libedp_b200.so"
+ABI_VERSION = 2  # EDP_ABI_VERSION in include/edp.h
 
 I64 = ctypes.c_int64
 I32 = ctypes.c_int32
@@ -86,6 +87,9 @@ def load():
     lib.edp_last_cuda_error.restype = ctypes.c_int
     lib.edp_last_error_site.restype = ctypes.c_char_p
     lib.edp_abi_version.restype = ctypes.c_int
+    if lib.edp_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{LIBRARY.name} has ABI version {lib.edp_abi_version()}, this "
+                           f"package needs {ABI_VERSION}: rebuild it (build.py)")
     _lib = lib
     return lib
 

@@ -46,6 +46,7 @@ enum edp_status {
 enum {
   EDP_STATUS_SLOTS = 16,
   EDP_METRICS = 20,
+  EDP_ABI_VERSION = 2,
   EDP_ERR_BIT_POLYGON = 1,
   EDP_ERR_BIT_WORKER = 2,
   EDP_ERR_BIT_RESIDUAL = 4,
@@ -161,6 +162,8 @@ const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
 /* Source location ("file:line") of the CUDA call behind the last EDP_ERR_CUDA. */
 const char *edp_last_error_site(void);
+/* EDP_ABI_VERSION of the library: 2 since metrics[] holds 20 counters
+ * (heavy_noded_polygons added); 1 had 19. */
 int edp_abi_version(void);
 
 #ifdef __cplusplus

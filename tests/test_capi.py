@@ -32,6 +32,24 @@ def test_library_exports_every_declared_symbol():
     assert lib.edp_status_string(1) == b"invalid argument"
 
 
+
+def header_constant(name):
+    text = (ROOT / "include/edp.h").read_text()
+    return int(re.search(rf"\b{name}\s*=\s*(\d+)", text).group(1))
+
+
+def test_header_constants_match_the_host():
+    """The counter array and ABI version the header states are the ones the
+    Python host reads and the library reports."""
+    from peel_b200 import _lib
+    from peel_b200.events import METRIC_NAMES
+    from peel_b200.solver import METRIC_COUNT
+
+    assert header_constant("EDP_METRICS") == METRIC_COUNT == len(METRIC_NAMES)
+    assert header_constant("EDP_STATUS_SLOTS") == 16
+    assert header_constant("EDP_ABI_VERSION") == _lib.ABI_VERSION == _lib.load().edp_abi_version()
+
+
 def test_default_capacities_match_reference():
     import ctypes
 
