@@ -1,0 +1,419 @@
+"""Exact intersection splitting of a triangle scene (offline, on the CPU).
+
+    python -m peel_b200.resolve INPUT.json OUTPUT.json
+
+The peelers take resolved meshes: no two triangles may cross.  This is the
+camera-independent preprocessing that produces one
+(src/resolve_intersections.cpp:19-105): every triangle is split where other
+triangles meet it, in exact rational arithmetic, and each piece keeps its
+parent's provenance (`original_source_id`, `mesh_face_id`); the output scene
+carries the input triangles as `original_triangles` and writes coordinates
+as exact rational strings ("n/d"), like the reference.
+
+Construction (this module's own; the reference calls CGAL's autorefine):
+
+1. Candidate pairs come from a sweep over padded binary64 boxes; each pair's
+   contact is computed exactly: the part of each triangle on the other's
+   plane, intersected along the planes' common line.  Coplanar pairs must
+   not overlap with positive area (outside the contract, as in the
+   reference); their touching points are kept.
+2. A triangle whose interior a contact segment crosses is cut by the
+   segment's supporting line (in its own plane), so its pieces are convex.
+3. Every point created by a contact or a cut is inserted into every piece
+   edge it lies on, so pieces that meet along a contact share the same
+   edges exactly.  Where two triangles cross, the four pieces along the
+   crossing then share its edges, which makes them non-manifold edges: the
+   contours the resolved-mesh topology keeps (src/peel_common.h:100-123).
+4. A piece that stayed a triangle is written as is; any other piece is
+   written as a fan around its vertex average, in the parent's winding.
+
+Unlike the reference's importer, the input need not be a manifold: any
+triangle soup without coplanar overlaps is accepted.  Zero-area input
+triangles pass through unchanged.
+"""
+
+import json
+import sys
+import time
+from fractions import Fraction as Q
+
+import numpy as np
+
+
+class ResolveError(ValueError):
+    pass
+
+
+# ---------------------------------------------------------------- numbers
+
+
+def rational(x):
+    """A scene number as an exact rational: JSON numbers exactly, strings as
+    integers or "numerator/denominator" only (src/exact_geometry.cpp:5-39)."""
+    if isinstance(x, bool):
+        raise ResolveError(f"Expected a number: {x!r}")
+    if isinstance(x, float):
+        if not np.isfinite(x):
+            raise ResolveError("Nonfinite coordinate")
+        return Q(x)
+    if isinstance(x, int):
+        return Q(x)
+    s = str(x)
+    num, _, den = s.partition("/")
+
+    def integer(v):
+        body = v[1:] if v[:1] in "+-" else v
+        return body.isdigit() and body.isascii()
+
+    if not integer(num) or (den and not integer(den)) or (_ and not den):
+        raise ResolveError(f"Expected integer or rational string: {s}")
+    if den and int(den) == 0:
+        raise ResolveError("Zero rational denominator")
+    return Q(int(num), int(den) if den else 1)
+
+
+def text(q):
+    """An exact rational as the reference writes it: "n/d", "/1" for integers."""
+    return f"{q.numerator}/{q.denominator}"
+
+
+# ---------------------------------------------------------------- vectors
+
+
+def sub(a, b):
+    return (a[0] - b[0], a[1] - b[1], a[2] - b[2])
+
+
+def add(a, b):
+    return (a[0] + b[0], a[1] + b[1], a[2] + b[2])
+
+
+def scale(a, s):
+    return (a[0] * s, a[1] * s, a[2] * s)
+
+
+def dot(a, b):
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+
+def cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+ZERO = (Q(0), Q(0), Q(0))
+
+
+def on_open_segment(x, u, w):
+    """x strictly between u and w on the segment u-w."""
+    d = sub(w, u)
+    r = sub(x, u)
+    if cross(d, r) != ZERO:
+        return None
+    t = dot(r, d)
+    return t / dot(d, d) if 0 < t < dot(d, d) else None
+
+
+def collinear(u, w, x):
+    return cross(sub(w, u), sub(x, u)) == ZERO
+
+
+# ---------------------------------------------------------------- contacts
+
+
+class Face:
+    """One input triangle: exact vertices, plane (normal . p = offset)."""
+
+    def __init__(self, index, record):
+        self.index = index
+        self.record = record
+        vertices = record["vertices"]
+        if len(vertices) != 3 or any(len(v) != 3 for v in vertices):
+            raise ResolveError("Expected a triangle of 3D vertices")
+        self.v = tuple(tuple(rational(c) for c in p) for p in vertices)
+        self.normal = cross(sub(self.v[1], self.v[0]), sub(self.v[2], self.v[0]))
+        self.offset = dot(self.normal, self.v[0])
+        self.degenerate = self.normal == ZERO
+        self.cuts = []  # (p, r): supporting lines of contact segments crossing the interior
+
+    def plane(self, p):
+        return dot(self.normal, p) - self.offset
+
+    def on_boundary(self, p, r):
+        """The segment p-r lies on the line of one of this triangle's edges."""
+        return any(collinear(self.v[k], self.v[(k + 1) % 3], p)
+                   and collinear(self.v[k], self.v[(k + 1) % 3], r) for k in range(3))
+
+
+def plane_section(face, other):
+    """Points of `face` on `other`'s plane: None (strictly one side),
+    "coplanar", or a list of one or two distinct points."""
+    values = [other.plane(p) for p in face.v]
+    if all(v > 0 for v in values) or all(v < 0 for v in values):
+        return None
+    if all(v == 0 for v in values):
+        return "coplanar"
+    points = [face.v[k] for k in range(3) if values[k] == 0]
+    for k in range(3):
+        a, b = values[k], values[(k + 1) % 3]
+        if (a < 0 < b) or (b < 0 < a):
+            u, w = face.v[k], face.v[(k + 1) % 3]
+            points.append(add(u, scale(sub(w, u), a / (a - b))))
+    unique = []
+    for p in points:
+        if p not in unique:
+            unique.append(p)
+    return unique
+
+
+def dominant_axes(normal):
+    k = max(range(3), key=lambda i: abs(normal[i]))
+    return [i for i in range(3) if i != k]
+
+
+def coplanar_contact(fa, fb):
+    """Touching points of two coplanar triangles; raises on a positive-area
+    overlap (outside the resolved-mesh contract)."""
+    ax = dominant_axes(fa.normal)
+    flat = lambda p: (p[ax[0]], p[ax[1]])
+    ta, tb = [flat(p) for p in fa.v], [flat(p) for p in fb.v]
+    orient = lambda a, b, c: (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+    sa = 1 if orient(*ta) > 0 else -1
+    poly = [(p, q) for p, q in zip(tb, fb.v)]
+    for k in range(3):
+        a, b = ta[k], ta[(k + 1) % 3]
+        side = lambda p: sa * orient(a, b, p)
+        out = []
+        for i in range(len(poly)):
+            (p, p3), (q, q3) = poly[i], poly[(i + 1) % len(poly)]
+            sp, sq = side(p), side(q)
+            if sp >= 0:
+                out.append((p, p3))
+            if (sp > 0 > sq) or (sq > 0 > sp):
+                t = sp / (sp - sq)
+                x3 = add(p3, scale(sub(q3, p3), t))
+                out.append((flat(x3), x3))
+        poly = out
+        if not poly:
+            return []
+    area2 = sum(orient(poly[0][0], poly[i][0], poly[i + 1][0]) for i in range(1, len(poly) - 1))
+    if area2 != 0:
+        raise ResolveError(
+            f"Triangles {fa.record.get('id', fa.index)} and {fb.record.get('id', fb.index)} "
+            "overlap on one plane with positive area; coincident surfaces are outside the "
+            "resolved-mesh contract")
+    return [p3 for _, p3 in poly]
+
+
+def contact(fa, fb):
+    """Exact contact of two non-degenerate triangles: (points, segment or None)."""
+    sa = plane_section(fb, fa)
+    if sa is None:
+        return [], None
+    if sa == "coplanar":
+        return coplanar_contact(fa, fb), None
+    sb = plane_section(fa, fb)
+    if sb is None:
+        return [], None
+    line = cross(fa.normal, fb.normal)
+    ra = sorted((dot(line, p), p) for p in sa)
+    rb = sorted((dot(line, p), p) for p in sb)
+    lo = max(ra[0], rb[0])
+    hi = min(ra[-1], rb[-1])
+    if lo[0] > hi[0]:
+        return [], None
+    if lo[0] == hi[0]:
+        return [lo[1]], None
+    return [lo[1], hi[1]], (lo[1], hi[1])
+
+
+# ---------------------------------------------------------------- pieces
+
+
+def split(poly, p, r, normal):
+    """Both sides of the convex polygon `poly` (3D, in the plane with
+    `normal`) about the line p-r of that plane; parts without area dropped."""
+    d = sub(r, p)
+    side = [dot(cross(d, sub(v, p)), normal) for v in poly]
+    if all(s >= 0 for s in side) or all(s <= 0 for s in side):
+        return [poly]
+    left, right = [], []
+    n = len(poly)
+    for i in range(n):
+        u, w = poly[i], poly[(i + 1) % n]
+        su, sw = side[i], side[(i + 1) % n]
+        if su >= 0:
+            left.append(u)
+        if su <= 0:
+            right.append(u)
+        if (su > 0 > sw) or (sw > 0 > su):
+            x = add(u, scale(sub(w, u), su / (su - sw)))
+            left.append(x)
+            right.append(x)
+    return [part for part in (left, right) if len(part) >= 3 and area_vector(part) != ZERO]
+
+
+def area_vector(poly):
+    total = ZERO
+    for i in range(1, len(poly) - 1):
+        total = add(total, cross(sub(poly[i], poly[0]), sub(poly[i + 1], poly[0])))
+    return total
+
+
+def boxes(points):
+    a = np.array([[float(c) for c in p] for p in points], dtype=np.float64).reshape(-1, 3)
+    return a
+
+
+def candidate_pairs(lo, hi):
+    """Index pairs whose boxes overlap (sweep along x)."""
+    order = np.argsort(lo[:, 0], kind="stable")
+    slo, shi = lo[order], hi[order]
+    pairs = []
+    for k in range(len(order)):
+        end = np.searchsorted(slo[:, 0], shi[k, 0], side="right")
+        if end <= k + 1:
+            continue
+        rest = np.arange(k + 1, end)
+        keep = rest[np.all(slo[rest, 1:] <= shi[k, 1:], axis=1)
+                    & np.all(shi[rest, 1:] >= slo[k, 1:], axis=1)]
+        pairs.extend((int(order[k]), int(order[j])) for j in keep)
+    return pairs
+
+
+def resolve(data):
+    """The resolved scene (a new dict) and a summary of the preprocessing."""
+    start = time.perf_counter()
+    triangles = data["triangles"]
+    faces = [Face(i, t) for i, t in enumerate(triangles)]
+    import_seconds = time.perf_counter() - start
+    start = time.perf_counter()
+    live = [f for f in faces if not f.degenerate]
+    if live:
+        corners = np.stack([boxes(f.v) for f in live])
+        pad = 1e-9 * (np.abs(corners).max(axis=(1, 2)) + 1.0)
+        lo = corners.min(axis=1) - pad[:, None]
+        hi = corners.max(axis=1) + pad[:, None]
+        pairs = candidate_pairs(lo, hi)
+    else:
+        pairs = []
+    points = []  # every contact point and cut vertex: inserted into the edges it lies on
+    segments = 0
+    for a, b in pairs:
+        fa, fb = live[a], live[b]
+        found, segment = contact(fa, fb)
+        points.extend(found)
+        if segment is None:
+            continue
+        crossing = False
+        for f in (fa, fb):
+            if f.on_boundary(*segment):
+                continue
+            crossing = True
+            if not any(collinear(p, r, segment[0]) and collinear(p, r, segment[1])
+                       for p, r in f.cuts):
+                f.cuts.append(segment)
+        segments += crossing
+    pieces = {}
+    for f in live:
+        parts = [list(f.v)]
+        for p, r in f.cuts:
+            parts = [q for part in parts for q in split(part, p, r, f.normal)]
+        pieces[f.index] = parts
+        if f.cuts:
+            points.extend(v for part in parts for v in part)
+    unique = list(dict.fromkeys(points))
+    cloud = boxes(unique) if unique else np.zeros((0, 3))
+    out = []
+    cut_faces = sum(1 for f in live if f.cuts)
+    for f in faces:
+        record = f.record
+        source = record.get("original_source_id", record.get("id", f.index))
+        mesh_face = record.get("mesh_face_id", source)
+        if f.degenerate:
+            polygons = [list(f.v)]
+        else:
+            polygons = []
+            for part in pieces[f.index]:
+                polygons.append(insert_points(part, unique, cloud))
+        for poly in polygons:
+            for tri in fan(poly):
+                out.append({"id": len(out), "original_source_id": source,
+                            "mesh_face_id": mesh_face,
+                            "vertices": [[text(c) for c in p] for p in tri]})
+    refine_seconds = time.perf_counter() - start
+    summary = {
+        "method": "exact rational line splitting with shared-edge insertion",
+        "arithmetic": "exact rational constructions",
+        "input_triangles": len(triangles),
+        "output_triangles": len(out),
+        "intersection_segments": segments,
+        "cut_triangles": cut_faces,
+        "import_seconds": import_seconds,
+        "refinement_seconds": refine_seconds,
+        "positive_area_coincident_surfaces_supported": False,
+    }
+    result = dict(data)
+    result["triangles"] = out
+    if "original_triangles" not in result:
+        result["original_triangles"] = triangles
+    result["intersection_preprocessing"] = summary
+    return result, summary
+
+
+def insert_points(poly, points, cloud):
+    """`poly` with every point of `points` lying inside one of its edges
+    inserted there, in order along the edge."""
+    if not points:
+        return poly
+    corners = boxes(poly)
+    pad = 1e-9 * (np.abs(corners).max() + 1.0)
+    near = np.nonzero(np.all(cloud >= corners.min(0) - pad, axis=1)
+                      & np.all(cloud <= corners.max(0) + pad, axis=1))[0]
+    if len(near) == 0:
+        return poly
+    result = []
+    n = len(poly)
+    for i in range(n):
+        u, w = poly[i], poly[(i + 1) % n]
+        result.append(u)
+        inside = []
+        for k in near:
+            t = on_open_segment(points[k], u, w)
+            if t is not None:
+                inside.append((t, points[k]))
+        result.extend(p for _, p in sorted(inside))
+    return result
+
+
+def fan(poly):
+    """Triangles of a convex piece: itself when it is one, else a fan around
+    its vertex average (every boundary edge kept, no T-junctions)."""
+    if len(poly) == 3:
+        return [poly]
+    n = len(poly)
+    center = tuple(sum(p[c] for p in poly) / n for c in range(3))
+    return [[center, poly[i], poly[(i + 1) % n]] for i in range(n)]
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    if len(argv) != 2:
+        sys.stderr.write("python -m peel_b200.resolve INPUT.json OUTPUT.json\nExact "
+                         "camera-independent intersection splitting of a triangle scene.\n")
+        return 2
+    try:
+        with open(argv[0]) as f:
+            data = json.load(f)
+        result, summary = resolve(data)
+        with open(argv[1], "w") as f:
+            json.dump(result, f)
+            f.write("\n")
+    except (OSError, ValueError, KeyError, TypeError) as e:
+        sys.stderr.write(f"error: {e}\n")
+        return 1
+    print(json.dumps(summary))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
