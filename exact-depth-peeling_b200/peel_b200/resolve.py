@@ -229,6 +229,35 @@ def contact(fa, fb):
 # ---------------------------------------------------------------- pieces
 
 
+def shared_contact_only(live, corners, pairs):
+    """For each candidate pair, True when the two triangles can only meet in
+    the vertices they share exactly: some vertex of one lies clearly off the
+    other's plane, every such vertex on the same side, and the rest are
+    vertices of the other (a triangle meets a plane only in its points on
+    it).  False leaves the pair to the exact test.
+
+    "Clearly" is binary64 against a margin: coordinates rounded from exact
+    values (relative error u), differences, a cross product and a dot
+    product stay within about 600 u M^3 of the exact side value, M the
+    largest coordinate magnitude of the pair; the margin is 1e-12 M^3, and
+    pairs with M outside [1e-50, 1e50] are left to the exact test."""
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    done = np.zeros(len(pairs), dtype=bool)
+    for a_col, b_col in ((0, 1), (1, 0)):
+        A, B = corners[pairs[:, a_col]], corners[pairs[:, b_col]]
+        m = np.maximum(np.abs(A).max(axis=(1, 2)), np.abs(B).max(axis=(1, 2)))
+        trusted = (m >= 1e-50) & (m <= 1e50)
+        tol = (1e-12 * m ** 3)[:, None]
+        normal = np.cross(A[:, 1] - A[:, 0], A[:, 2] - A[:, 0])
+        side = np.einsum("kvj,kj->kv", B - A[:, :1], normal)
+        clear = (side > tol) | (side < -tol)
+        one_side = np.all(~clear | (side > 0), axis=1) | np.all(~clear | (side < 0), axis=1)
+        for k in np.nonzero(trusted & one_side & clear.any(axis=1) & ~done)[0]:
+            fa, fb = live[pairs[k, a_col]], live[pairs[k, b_col]]
+            done[k] = all(clear[k, v] or fb.v[v] in fa.v for v in range(3))
+    return done
+
+
 def split(poly, p, r, normal):
     """Both sides of the convex polygon `poly` (3D, in the plane with
     `normal`) about the line p-r of that plane; parts without area dropped."""
@@ -294,14 +323,16 @@ def resolve(data):
         lo = corners.min(axis=1) - pad[:, None]
         hi = corners.max(axis=1) + pad[:, None]
         pairs = candidate_pairs(lo, hi)
+        skip = shared_contact_only(live, corners, pairs)
+        pairs = [pq for pq, gone in zip(pairs, skip) if not gone]
     else:
         pairs = []
-    points = []  # every contact point and cut vertex: inserted into the edges it lies on
+    points = []  # contact points and cut vertices: inserted into the edges they lie on
     segments = 0
     for a, b in pairs:
         fa, fb = live[a], live[b]
         found, segment = contact(fa, fb)
-        points.extend(found)
+        points.extend(x for x in found if not (x in fa.v and x in fb.v))
         if segment is None:
             continue
         crossing = False
@@ -320,7 +351,7 @@ def resolve(data):
             parts = [q for part in parts for q in split(part, p, r, f.normal)]
         pieces[f.index] = parts
         if f.cuts:
-            points.extend(v for part in parts for v in part)
+            points.extend(v for part in parts for v in part if v not in f.v)
     unique = list(dict.fromkeys(points))
     cloud = boxes(unique) if unique else np.zeros((0, 3))
     out = []
@@ -371,13 +402,19 @@ def insert_points(poly, points, cloud):
                       & np.all(cloud <= corners.max(0) + pad, axis=1))[0]
     if len(near) == 0:
         return poly
+    # Points clearly off an edge's line (binary64 cross product above a
+    # margin far over its rounding error, as in shared_contact_only) skip the
+    # exact test.
+    tol = 1e-12 * float(max(np.abs(corners).max(), np.abs(cloud[near]).max())) ** 2
     result = []
     n = len(poly)
     for i in range(n):
         u, w = poly[i], poly[(i + 1) % n]
         result.append(u)
+        fu, fw = corners[i], corners[(i + 1) % n]
+        off = np.abs(np.cross(fw - fu, cloud[near] - fu)).max(axis=1)
         inside = []
-        for k in near:
+        for k in near[off <= tol]:
             t = on_open_segment(points[k], u, w)
             if t is not None:
                 inside.append((t, points[k]))

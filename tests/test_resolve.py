@@ -225,6 +225,17 @@ def test_coplanar_overlap_rejected(name):
         resolve(parity.fixture(name))
 
 
+def test_duplicate_triangle_rejected():
+    """A triangle listed twice overlaps itself on one plane: it is an error,
+    not a pair whose shared vertices are its only contact."""
+    from peel_b200.resolve import ResolveError
+
+    data = parity.fixture("single")
+    twice = dict(data, triangles=data["triangles"] + [dict(data["triangles"][0], id=99)])
+    with pytest.raises(ResolveError, match="positive area"):
+        resolve(twice)
+
+
 def test_numbers_parse_like_the_reference():
     from peel_b200.resolve import ResolveError, rational, text
 
