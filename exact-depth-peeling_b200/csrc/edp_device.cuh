@@ -54,7 +54,7 @@ __host__ __device__ inline V2 operator/(V2 a, double s) { return V2{a.x / s, a.y
 __host__ __device__ inline bool operator==(V2 a, V2 b) { return a.x == b.x && a.y == b.y; }
 __host__ __device__ inline bool operator!=(V2 a, V2 b) { return !(a == b); }
 __host__ __device__ inline double dot(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
-__device__ inline double length(V2 a) { return sqrt(a.x * a.x + a.y * a.y); }
+__host__ __device__ inline double length(V2 a) { return sqrt(a.x * a.x + a.y * a.y); }
 // Lexicographic order of points (event_kernels.py:66-68).
 __host__ __device__ inline bool less(V2 a, V2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
 
@@ -69,12 +69,15 @@ struct Plane { double a, b, c, pad; };
 __host__ __device__ inline double value(const Plane &s, V2 x) { return s.a * x.x + s.b * x.y + s.c; }
 
 // ---------------------------------------------------------------- polygons
+// The polygon helpers below are host and device functions so that the CPU
+// tests can run the kernels' own code (binary64 without contraction rounds
+// the same on both).
 // Remove near-duplicate points and collapse slivers (kernels.py:146-176):
 // points closer than EPS/100 merge, and a translation-stable area/perimeter
 // test drops polygons narrower than about EPS.  Returns the new size (0 when
 // the polygon collapsed); sizes above kMaxVertices are returned unchanged so
 // that the caller can raise the polygon-capacity error.
-__device__ inline int clean(V2 *p, int n) {
+__host__ __device__ inline int clean(V2 *p, int n) {
   if (n > kMaxVertices) return n;
   int count = 0;
   const double merge = kEps * 0.01;
@@ -95,7 +98,7 @@ __device__ inline int clean(V2 *p, int n) {
   return count;
 }
 
-__device__ inline int append(V2 *p, int n, V2 x) {
+__host__ __device__ inline int append(V2 *p, int n, V2 x) {
   if (n < kMaxVertices) p[n] = x;
   return n + 1;
 }
@@ -103,8 +106,8 @@ __device__ inline int append(V2 *p, int n, V2 x) {
 // Split a convex polygon by the line s(x - anchor) = 0 into the part with
 // s >= 0 (inside) and s <= 0 (outside), then clean both (kernels.py:184-203).
 // Evaluating relative to the anchor keeps short clipping edges in place.
-__device__ inline void split_at(const V2 *p, int n, const Plane &s, V2 anchor, V2 *in, int &ni,
-                                V2 *out, int &no) {
+__host__ __device__ inline void split_at(const V2 *p, int n, const Plane &s, V2 anchor, V2 *in,
+                                         int &ni, V2 *out, int &no) {
   ni = 0;
   no = 0;
   for (int j = 0; j < n; ++j) {
@@ -123,15 +126,15 @@ __device__ inline void split_at(const V2 *p, int n, const Plane &s, V2 anchor, V
 }
 
 // Split by the supporting line of edge a->b: inside is to the left.
-__device__ inline void split_edge(const V2 *p, int n, V2 a, V2 b, V2 *in, int &ni, V2 *out,
-                                  int &no) {
+__host__ __device__ inline void split_edge(const V2 *p, int n, V2 a, V2 b, V2 *in, int &ni,
+                                           V2 *out, int &no) {
   V2 d = b - a;
   Plane s{-d.y, d.x, 0.0, 0.0};
   split_at(p, n, s, a, in, ni, out, no);
 }
 
 // Some edge of a has no vertex of b strictly on its left (kernels.py:219-232).
-__device__ inline bool separated(const V2 *a, int na, const V2 *b, int nb) {
+__host__ __device__ inline bool separated(const V2 *a, int na, const V2 *b, int nb) {
   for (int j = 0; j < na; ++j) {
     bool positive = false;
     for (int k = 0; k < nb; ++k)
