@@ -244,18 +244,27 @@ def shared_contact_only(live, corners, pairs):
     pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
     done = np.zeros(len(pairs), dtype=bool)
     for a_col, b_col in ((0, 1), (1, 0)):
-        A, B = corners[pairs[:, a_col]], corners[pairs[:, b_col]]
-        m = np.maximum(np.abs(A).max(axis=(1, 2)), np.abs(B).max(axis=(1, 2)))
-        trusted = (m >= 1e-50) & (m <= 1e50)
-        tol = (1e-12 * m ** 3)[:, None]
-        normal = np.cross(A[:, 1] - A[:, 0], A[:, 2] - A[:, 0])
-        side = np.einsum("kvj,kj->kv", B - A[:, :1], normal)
-        clear = (side > tol) | (side < -tol)
-        one_side = np.all(~clear | (side > 0), axis=1) | np.all(~clear | (side < 0), axis=1)
+        with np.errstate(over="ignore", invalid="ignore"):  # untrusted pairs are discarded
+            trusted, side, tol = _sides(corners, pairs, a_col, b_col)
+            clear = (side > tol) | (side < -tol)
+            one_side = (np.all(~clear | (side > 0), axis=1)
+                        | np.all(~clear | (side < 0), axis=1))
         for k in np.nonzero(trusted & one_side & clear.any(axis=1) & ~done)[0]:
             fa, fb = live[pairs[k, a_col]], live[pairs[k, b_col]]
             done[k] = all(clear[k, v] or fb.v[v] in fa.v for v in range(3))
     return done
+
+
+def _sides(corners, pairs, a_col, b_col):
+    """Binary64 side values of each pair's second triangle against the
+    first one's plane, their margin, and whether the pair's range is trusted."""
+    A, B = corners[pairs[:, a_col]], corners[pairs[:, b_col]]
+    m = np.maximum(np.abs(A).max(axis=(1, 2)), np.abs(B).max(axis=(1, 2)))
+    trusted = (m >= 1e-50) & (m <= 1e50)
+    tol = (1e-12 * m ** 3)[:, None]
+    normal = np.cross(A[:, 1] - A[:, 0], A[:, 2] - A[:, 0])
+    side = np.einsum("kvj,kj->kv", B - A[:, :1], normal)
+    return trusted, side, tol
 
 
 def split(poly, p, r, normal):
@@ -404,15 +413,17 @@ def insert_points(poly, points, cloud):
         return poly
     # Points clearly off an edge's line (binary64 cross product above a
     # margin far over its rounding error, as in shared_contact_only) skip the
-    # exact test.
-    tol = 1e-12 * float(max(np.abs(corners).max(), np.abs(cloud[near]).max())) ** 2
+    # exact test; outside [1e-50, 1e50] every point takes it.
+    m = float(max(np.abs(corners).max(), np.abs(cloud[near]).max()))
+    tol = 1e-12 * m ** 2 if 1e-50 <= m <= 1e50 else np.inf
     result = []
     n = len(poly)
     for i in range(n):
         u, w = poly[i], poly[(i + 1) % n]
         result.append(u)
         fu, fw = corners[i], corners[(i + 1) % n]
-        off = np.abs(np.cross(fw - fu, cloud[near] - fu)).max(axis=1)
+        with np.errstate(over="ignore", invalid="ignore"):  # out of range: tol is inf
+            off = np.abs(np.cross(fw - fu, cloud[near] - fu)).max(axis=1)
         inside = []
         for k in near[off <= tol]:
             t = on_open_segment(points[k], u, w)

@@ -225,6 +225,28 @@ def test_coplanar_overlap_rejected(name):
         resolve(parity.fixture(name))
 
 
+@pytest.mark.parametrize("exponent", [500, -500])
+def test_extreme_scales_resolve_exactly(exponent):
+    """Coordinates scaled by 2^500 or 2^-500 (outside the range the binary64
+    pre-tests trust) resolve to exactly the scaled pieces."""
+    import warnings
+
+    k = Q(2) ** exponent
+    for name in ("crossing", "random_07"):
+        data = parity.fixture(name)
+        scaled = dict(data, triangles=[
+            dict(t, vertices=[[str(Q(c) * k) for c in v] for v in t["vertices"]])
+            for t in data["triangles"]])
+        with warnings.catch_warnings():
+            warnings.simplefilter("error")
+            big, _ = resolve(scaled)
+        small, _ = resolve(data)
+        grow = lambda r: sorted((t["original_source_id"], tuple(
+            tuple(Q(c) * k for c in p) for p in tri(t))) for t in r["triangles"])
+        same = lambda r: sorted((t["original_source_id"], tri(t)) for t in r["triangles"])
+        assert same(big) == grow(small)
+
+
 def test_duplicate_triangle_rejected():
     """A triangle listed twice overlaps itself on one plane: it is an error,
     not a pair whose shared vertices are its only contact."""
