@@ -2,7 +2,7 @@
 
 Run once in a container where the reference checkout is mounted:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py REFERENCE_CHECKOUT
 
 It copies two kinds of data (no code) out of the reference:
 
@@ -95,4 +95,6 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT")
+    main(sys.argv[1])
