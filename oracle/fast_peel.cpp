@@ -636,8 +636,16 @@ struct Totals {
   int64_t layers = 0, patches = 0, faces = 0, residual = 0;
 };
 
+// One output region: its layer, the input face it comes from, and its ring
+// on the 2^bits grid.
+struct Region {
+  int layer, face;
+  Ring ring;
+};
+
 // The all-layer scheduler (peel_common.h:341-460) with the accelerated path.
-Totals extract(const Scene &s, int layers, int threads) {
+// With `regions`, every layer's convex regions are also collected.
+Totals extract(const Scene &s, int layers, int threads, std::vector<Region> *regions = nullptr) {
   Policy p{s};
   std::vector<Patch> originals;
   for (size_t i = 0; i < s.sources.size(); ++i) originals.push_back({int(i), s.sources[i].initial});
@@ -683,6 +691,9 @@ Totals extract(const Scene &s, int layers, int threads) {
       for (auto &r : work[i].hidden) next.push_back({residual[i].source, std::move(r)});
     }
     if (layer.empty()) throw std::runtime_error("BVH peeling made no progress");
+    if (regions)
+      for (const Patch &patch : layer)
+        regions->push_back({k, s.sources[patch.source].id, patch.points});
     auto faces = mesh(layer, threads);
     t.layers += 1;
     t.patches += int64_t(layer.size());
@@ -716,6 +727,43 @@ int fastpeel_run(const double *vertices, const int32_t *faces, int64_t nf, const
     out[1] = t.patches;
     out[2] = t.faces;
     out[3] = t.residual;
+    return 0;
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+
+// One extraction that also returns its regions: meta[3 * i] = layer, input
+// face and vertex count of region i, coords[2 * j] the grid coordinates of
+// its vertices (region after region).  out[0..1] receive the region and
+// vertex counts; when either exceeds its capacity nothing is written to meta
+// or coords and the call returns 1 (call again with larger buffers).  out[2]
+// receives the layer count.  Returns 0, 1, or -1 on an algorithm error.
+int fastpeel_regions(const double *vertices, const int32_t *faces, int64_t nf,
+                     const double *camera, const double *settings, int32_t threads, int32_t bits,
+                     int32_t resolved, int32_t layers, int64_t region_capacity,
+                     int64_t vertex_capacity, int64_t *meta, int64_t *coords, int64_t *out) {
+  try {
+    Scene s = read(vertices, faces, nf, camera, settings, bits, resolved != 0);
+    std::vector<Region> regions;
+    Totals t = extract(s, layers, threads, &regions);
+    int64_t count = 0;
+    for (const Region &r : regions) count += int64_t(r.ring.size());
+    out[0] = int64_t(regions.size());
+    out[1] = count;
+    out[2] = t.layers;
+    if (out[0] > region_capacity || count > vertex_capacity) return 1;
+    int64_t j = 0;
+    for (size_t i = 0; i < regions.size(); ++i) {
+      meta[3 * i] = regions[i].layer;
+      meta[3 * i + 1] = regions[i].face;
+      meta[3 * i + 2] = int64_t(regions[i].ring.size());
+      for (Point v : regions[i].ring) {
+        coords[2 * j] = v.x;
+        coords[2 * j + 1] = v.y;
+        ++j;
+      }
+    }
     return 0;
   } catch (const std::exception &) {
     return -1;
