@@ -173,6 +173,234 @@ def audit(peeler, labels, data, samples=512, queries=()):
     return report
 
 
+VERTEX_SCOPE = ("Sampled output polygon vertices against the exact rational intersection of "
+                "the two projected source-edge (or window) lines their incident edges lie on; "
+                "errors in normalised window units and relative to the projected scene extent.")
+
+
+class ExactOutlines:
+    """Exact projected outlines of a mesh's triangles, built on demand.
+
+    The inputs are the peeler's own binary64 arrays (vertices [V,3], faces
+    [N,3], the 4x4 affine world-to-camera matrix and the six settings: window
+    xmin, ymin, xmax, ymax, perspective flag, near).  Every double is taken
+    exactly.  A triangle's outline is its camera-space polygon clipped to
+    z >= near (perspective only), projected (x/z, y/z) or (x, y), and mapped
+    to the normalised window; its edges, with the window's four borders, are
+    every line a vertex of an analytic depth peel can lie on (contour cuts run
+    along source edges).  Binary64 boxes of the projections, padded, select
+    the triangles near a query."""
+
+    def __init__(self, vertices, faces, camera, settings):
+        self.vertices = np.asarray(vertices, dtype=np.float64).reshape(-1, 3)
+        self.faces = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+        camera = np.asarray(camera, dtype=np.float64).reshape(4, 4)
+        settings = np.asarray(settings, dtype=np.float64).reshape(-1)
+        self.matrix = [[Q(float(x)) for x in camera[r]] for r in range(3)]
+        self.perspective = bool(settings[4] != 0)
+        self.near = Q(float(settings[5]))
+        self.window = [Q(float(x)) for x in settings[:4]]
+        self._cam = {}
+        self._outline = {}
+        self._plane = {}
+        cam = self.vertices @ camera[:3, :3].T + camera[:3, 3]
+        tri = cam[self.faces]
+        if self.perspective:
+            z = tri[:, :, 2]
+            crosses = ~(z > settings[5]).all(axis=1)
+            xy = tri[:, :, :2] / np.where(z > 0, z, 1.0)[:, :, None]
+        else:
+            crosses = np.zeros(len(tri), bool)
+            xy = tri[:, :, :2]
+        uv = (xy - settings[:2]) / (settings[2:4] - settings[:2])
+        lo, hi = uv.min(axis=1), uv.max(axis=1)
+        pad = 1e-7 * (1.0 + np.abs(lo).max(axis=1, initial=0) + np.abs(hi).max(axis=1, initial=0))
+        self.lo = lo - pad[:, None]
+        self.hi = hi + pad[:, None]
+        # A triangle that reaches behind the near plane projects without a
+        # finite binary64 box: it is a candidate everywhere.
+        self.lo[crosses] = -np.inf
+        self.hi[crosses] = np.inf
+        visible = ~crosses
+        if visible.any():
+            self.extent = float(max(hi[visible].max(axis=0) - lo[visible].min(axis=0)))
+        else:
+            self.extent = 1.0
+
+    def _camera_point(self, index):
+        if index not in self._cam:
+            p = [Q(float(x)) for x in self.vertices[index]]
+            self._cam[index] = tuple(row[0] * p[0] + row[1] * p[1] + row[2] * p[2] + row[3]
+                                     for row in self.matrix)
+        return self._cam[index]
+
+    def _normalise(self, c):
+        if self.perspective:
+            x, y = c[0] / c[2], c[1] / c[2]
+        else:
+            x, y = c[0], c[1]
+        w = self.window
+        return ((x - w[0]) / (w[2] - w[0]), (y - w[1]) / (w[3] - w[1]))
+
+    def outline(self, face):
+        """Exact normalised outline of `face` (a list of (u, v) Fractions)."""
+        if face not in self._outline:
+            ring = [self._camera_point(int(i)) for i in self.faces[face]]
+            if self.perspective:
+                clipped = []
+                for k, a in enumerate(ring):
+                    b = ring[(k + 1) % len(ring)]
+                    if a[2] >= self.near:
+                        clipped.append(a)
+                    if (a[2] >= self.near) != (b[2] >= self.near):
+                        t = (self.near - a[2]) / (b[2] - a[2])
+                        clipped.append(tuple(a[j] + t * (b[j] - a[j]) for j in range(3)))
+                ring = [c for c in clipped if c[2] > 0]
+            self._outline[face] = [self._normalise(c) for c in ring]
+        return self._outline[face]
+
+    def plane(self, face):
+        """Exact depth score of `face` as an affine function a*u + b*v + c of
+        the normalised window point (the score is z for an orthographic
+        camera and 1/z for a pinhole one, both affine in the projection), or
+        None when the triangle projects to a segment or a point."""
+        if face not in self._plane:
+            ring = [self._camera_point(int(i)) for i in self.faces[face]]
+            uv = [self._normalise(c) for c in ring] if all(c[2] != 0 for c in ring) \
+                or not self.perspective else None
+            result = None
+            if uv is not None:
+                score = [1 / c[2] if self.perspective else c[2] for c in ring]
+                (u0, v0), (u1, v1), (u2, v2) = uv
+                det = (u1 - u0) * (v2 - v0) - (u2 - u0) * (v1 - v0)
+                if det != 0:
+                    ds1, ds2 = score[1] - score[0], score[2] - score[0]
+                    a = (ds1 * (v2 - v0) - ds2 * (v1 - v0)) / det
+                    b = ((u1 - u0) * ds2 - (u2 - u0) * ds1) / det
+                    result = (a, b, score[0] - a * u0 - b * v0)
+            self._plane[face] = result
+        return self._plane[face]
+
+    def lines_near(self, lo, hi, face=None):
+        """Exact lines (pairs of distinct exact points) of every outline whose
+        box meets the box [lo, hi], plus the window borders and, with `face`,
+        the lines where `face`'s depth equals each of those triangles' (the
+        iterative clipping route cuts along them)."""
+        hit = np.nonzero((self.lo[:, 0] <= hi[0]) & (self.hi[:, 0] >= lo[0])
+                         & (self.lo[:, 1] <= hi[1]) & (self.hi[:, 1] >= lo[1]))[0]
+        one, zero = Q(1), Q(0)
+        lines = [((zero, zero), (one, zero)), ((one, zero), (one, one)),
+                 ((one, one), (zero, one)), ((zero, one), (zero, zero))]
+        own = self.plane(face) if face is not None else None
+        for f in hit:
+            ring = self.outline(int(f))
+            for k in range(len(ring)):
+                a, b = ring[k], ring[(k + 1) % len(ring)]
+                if a != b:
+                    lines.append((a, b))
+            other = self.plane(int(f)) if own is not None and int(f) != face else None
+            if other is not None:
+                da, db, dc = (x - y for x, y in zip(own, other))
+                if db != 0:
+                    lines.append(((zero, -dc / db), (one, -(da + dc) / db)))
+                elif da != 0:
+                    lines.append(((-dc / da, zero), (-dc / da, one)))
+        return lines
+
+
+def _best_line(lines, floats, p, q):
+    """Index of the line nearest to both float points p and q, and that
+    distance (the larger of the two, in normalised units)."""
+    a, d = floats[:, 0:2], floats[:, 2:4] - floats[:, 0:2]
+    length = np.maximum(np.hypot(d[:, 0], d[:, 1]), 1e-300)
+    dp = np.abs(d[:, 0] * (p[1] - a[:, 1]) - d[:, 1] * (p[0] - a[:, 0])) / length
+    dq = np.abs(d[:, 0] * (q[1] - a[:, 1]) - d[:, 1] * (q[0] - a[:, 0])) / length
+    worst = np.maximum(dp, dq)
+    k = int(np.argmin(worst))
+    return k, float(worst[k])
+
+
+def _intersection(l1, l2):
+    """Exact intersection point of two lines given by exact point pairs, or
+    None when they are parallel."""
+    (a, b), (c, d) = l1, l2
+    r = (b[0] - a[0], b[1] - a[1])
+    s = (d[0] - c[0], d[1] - c[1])
+    den = r[0] * s[1] - r[1] * s[0]
+    if den == 0:
+        return None
+    t = ((c[0] - a[0]) * s[1] - (c[1] - a[1]) * s[0]) / den
+    return (a[0] + t * r[0], a[1] + t * r[1])
+
+
+def vertex_audit(polygons, sources, outlines, samples=512, seed=0, tolerance=1e-7):
+    """Exact error of sampled output polygon vertices.
+
+    `polygons` are (k, 2) float arrays in the normalised window, `sources`
+    their dense face indices into `outlines` (an ExactOutlines).  For each
+    sampled polygon, every vertex's two incident edges are matched to the
+    exact line nearest to both of their endpoints - a source edge, a window
+    border or a line of equal depth between the polygon's source and another
+    triangle whose box meets the source's; the vertex's
+    exact position is those lines' rational intersection.  A vertex whose
+    edges match no line within `tolerance`, or whose two edges match one line
+    (a collinear vertex), is counted and not measured.  Returns a report with
+    the maximum absolute error (normalised window units, per coordinate) and
+    that maximum relative to the projected scene's extent."""
+    count = len(polygons)
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(count, size=min(samples, count), replace=False) if count else []
+    measured = collinear = unexplained = 0
+    worst = 0.0
+    worst_example = None
+    for i in picks:
+        v = np.asarray(polygons[i], dtype=np.float64)
+        n = len(v)
+        if n < 3:
+            continue
+        face = int(sources[i])
+        lines = outlines.lines_near(outlines.lo[face], outlines.hi[face], face) \
+            if np.isfinite(outlines.lo[face]).all() else \
+            outlines.lines_near(v.min(0) - 1e-7, v.max(0) + 1e-7, face)
+        floats = np.array([[float(a[0]), float(a[1]), float(b[0]), float(b[1])]
+                           for a, b in lines])
+        fitted = [_best_line(lines, floats, v[k], v[(k + 1) % n]) for k in range(n)]
+        for k in range(n):
+            (l_in, d_in), (l_out, d_out) = fitted[k - 1], fitted[k]
+            if max(d_in, d_out) > tolerance:
+                unexplained += 1
+                continue
+            point = _intersection(lines[l_in], lines[l_out])
+            if point is None:
+                collinear += 1
+                continue
+            err = float(max(abs(Q(float(v[k, 0])) - point[0]),
+                            abs(Q(float(v[k, 1])) - point[1])))
+            measured += 1
+            if err > worst:
+                worst = err
+                worst_example = {"polygon": int(i), "vertex": int(k), "source": face,
+                                 "uv": v[k].tolist(),
+                                 "exact": [float(point[0]), float(point[1])]}
+    return {"scope": VERTEX_SCOPE, "polygons": int(len(picks)), "vertices_measured": measured,
+            "collinear_vertices": collinear, "unexplained_vertices": unexplained,
+            "max_abs_error": worst, "scene_extent": outlines.extent,
+            "max_rel_error": worst / outlines.extent, "worst": worst_example}
+
+
+def peeler_vertex_audit(peeler, samples=512, seed=0):
+    """vertex_audit of a finished extraction, against its own input arrays."""
+    info = peeler.read_status()
+    count = info["polygons"]
+    n = peeler.output.sizes[:count].cpu().numpy()
+    v = peeler.output.vertices[:count].cpu().numpy()
+    src = peeler.output_sources[:count].cpu().numpy()
+    keep = np.nonzero(n >= 3)[0]
+    outlines = ExactOutlines(peeler.vertices.cpu().numpy(), peeler.faces.cpu().numpy(),
+                             peeler.camera.cpu().numpy(), peeler.settings.cpu().numpy())
+    return vertex_audit([v[i, : n[i]] for i in keep], src[keep], outlines, samples, seed)
+
+
 def main(argv=None):
     from . import DevicePeeler, EventPeeler
     from .io import load_scene
