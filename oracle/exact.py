@@ -778,14 +778,21 @@ class SparseRanks:
         # query must consider them.
         self.always = np.nonzero(~front)[0].tolist()
         self.cells = cells
-        clo = np.clip(np.floor(lo * cells), 0, cells - 1).astype(np.int64)
-        chi = np.clip(np.floor(hi * cells), 0, cells - 1).astype(np.int64)
-        self.grid: dict = {}
         self.lo, self.hi = lo, hi
-        for f in np.nonzero(front)[0]:
-            for cx in range(clo[f, 0], chi[f, 0] + 1):
-                for cy in range(clo[f, 1], chi[f, 1] + 1):
-                    self.grid.setdefault((cx, cy), []).append(int(f))
+        # A compressed uniform grid: the faces meeting each cell, cell by cell.
+        faces = np.nonzero(front)[0]
+        clo = np.clip(np.floor(lo[faces] * cells), 0, cells - 1).astype(np.int64)
+        chi = np.clip(np.floor(hi[faces] * cells), 0, cells - 1).astype(np.int64)
+        nx, ny = chi[:, 0] - clo[:, 0] + 1, chi[:, 1] - clo[:, 1] + 1
+        per = nx * ny
+        owner = np.repeat(np.arange(len(faces)), per)
+        local = np.arange(int(per.sum())) - np.repeat(np.cumsum(per) - per, per)
+        cx = clo[owner, 0] + local % nx[owner]
+        cy = clo[owner, 1] + local // nx[owner]
+        cell = cx * cells + cy
+        order = np.argsort(cell, kind="stable")
+        self.cell_faces = faces[owner[order]]
+        self.cell_start = np.searchsorted(cell[order], np.arange(cells * cells + 1))
 
     def source(self, f):
         """(score, exact ccw polygon) of face f, or None if it projects to nothing."""
@@ -799,9 +806,11 @@ class SparseRanks:
         return self.cache[f]
 
     def candidates(self, u, v):
+        u, v = float(u), float(v)
         cx = min(self.cells - 1, max(0, int(u * self.cells)))
         cy = min(self.cells - 1, max(0, int(v * self.cells)))
-        out = [f for f in self.grid.get((cx, cy), [])
+        c = cx * self.cells + cy
+        out = [int(f) for f in self.cell_faces[self.cell_start[c]:self.cell_start[c + 1]]
                if self.lo[f, 0] <= u <= self.hi[f, 0] and self.lo[f, 1] <= v <= self.hi[f, 1]]
         return out + self.always
 
@@ -847,3 +856,51 @@ class SparseRanks:
             if r is not None:
                 return r
         return None
+
+
+# --------------------------------------------------------------------------
+# Parallel sampled ranks (a process pool of SparseRanks over one mesh)
+
+_POOL_MESHES = None
+_POOL_RANKS: dict = {}
+
+
+def _pool_init(hosts):
+    global _POOL_MESHES
+    _POOL_MESHES = hosts
+
+
+def _pool_rank(item):
+    mesh, face, ring = item
+    if mesh not in _POOL_RANKS:
+        _POOL_RANKS[mesh] = SparseRanks(*_POOL_MESHES[mesh])
+    return _POOL_RANKS[mesh].polygon_rank(face, ring)
+
+
+def polygon_ranks_multi(hosts, items, processes=None):
+    """Exact ranks of (mesh, face, ring) items, ``mesh`` indexing ``hosts``
+    (each (vertices, faces, camera, settings)), each as
+    ``SparseRanks.polygon_rank``, over a pool of spawned processes (spawned,
+    so that the pool is safe after a CUDA context exists in the caller)."""
+    import multiprocessing
+    import os
+
+    items = list(items)
+    if processes is None:
+        processes = min(16, os.cpu_count() or 1)
+    if processes <= 1 or len(items) < 64:
+        cache = {}
+        out = []
+        for mesh, face, ring in items:
+            if mesh not in cache:
+                cache[mesh] = SparseRanks(*hosts[mesh])
+            out.append(cache[mesh].polygon_rank(face, ring))
+        return out
+    ctx = multiprocessing.get_context("spawn")
+    with ctx.Pool(processes, initializer=_pool_init, initargs=(list(hosts),)) as pool:
+        return pool.map(_pool_rank, items, chunksize=max(1, len(items) // (8 * processes)))
+
+
+def polygon_ranks(host, items, processes=None):
+    """polygon_ranks_multi on one mesh: items are (face, ring)."""
+    return polygon_ranks_multi([host], [(0, f, r) for f, r in items], processes)
