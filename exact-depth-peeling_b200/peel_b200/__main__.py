@@ -1,9 +1,13 @@
-"""JSON upload and explicit NPZ download around a device-resident extraction.
+"""Peel a scene JSON on the GPU and write its triangle layers.
 
-    python -m peel_b200 scene.json --method events --out layers.npz
+    python -m peel_b200 scene.json --out layers.npz [--method peel|events]
+                        [--layers K] [--pool-scale S] [--pieces P] [--device cuda:0]
 
-Writes ``uv``, ``world``, ``sources`` (external ids) and zero-based ``layers``
-plus a JSON sidecar, like warp_peel/__main__.py:13-77.
+``layers.npz`` holds ``uv``, ``world``, ``sources`` (external ids) and
+zero-based ``layers``; ``layers.json`` beside it records the method, the
+scene and the decoded status.  Flags, file names and sidecar keys are the
+reference's command line (warp_peel/__main__.py), which readers of these
+files depend on.
 """
 
 import argparse
@@ -16,49 +20,66 @@ import numpy as np
 from . import Capacities, DevicePeeler, EventCapacities, EventPeeler
 from .io import download_mesh, load_scene
 
+SIDECAR_FORMAT = "warp-peel-approximate-v1"
 
-def main(argv=None):
-    parser = argparse.ArgumentParser(description=__doc__)
+# Per method: the peeler, its capacity type, and the pools --pool-scale grows.
+METHODS = {
+    "peel": (DevicePeeler, Capacities, ("residual", "polygons", "vertices", "triangles")),
+    "events": (EventPeeler, EventCapacities,
+               ("frontier", "regions", "hits", "vertices", "triangles")),
+}
+
+
+def parse(argv):
+    parser = argparse.ArgumentParser(prog="python -m peel_b200", description=__doc__,
+                                     formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("scene", type=Path)
     parser.add_argument("--out", type=Path, required=True)
     parser.add_argument("--layers", type=int, default=0, help="0 means all layers")
-    parser.add_argument("--method", choices=("peel", "events"), default="peel",
-                        help="events selects contour subdivision with shared ray ranks")
-    parser.add_argument("--pieces", type=int)
-    parser.add_argument("--pool-scale", type=int, default=1)
+    parser.add_argument("--method", choices=tuple(METHODS), default="peel",
+                        help="peel: iterative per-layer clipping; events: contour "
+                             "subdivision with shared ray ranks")
+    parser.add_argument("--pieces", type=int, help="piece budget per clipping task (peel)")
+    parser.add_argument("--pool-scale", type=int, default=1,
+                        help="multiply the output and work pools by this factor")
     parser.add_argument("--device", default="cuda:0")
     args = parser.parse_args(argv)
+    if args.pieces is not None and args.method != "peel":
+        parser.error("--pieces applies only to --method peel")
+    return args
+
+
+def capacities(args, faces):
+    """The method's default capacities for `faces` sources, scaled and
+    overridden as the flags ask."""
+    _, kind, scaled = METHODS[args.method]
+    base = kind.for_mesh(faces)
+    changes = {name: getattr(base, name) * args.pool_scale for name in scaled}
+    if args.pieces:  # 0 keeps the default, as in the reference
+        changes["pieces_per_worker"] = args.pieces
+    return replace(base, **changes)
+
+
+def sidecar(args, status):
+    return {"format": SIDECAR_FORMAT, "zero_based_layers": True, "exact_geometry": False,
+            "method": args.method, "scene": str(args.scene), "output": status}
+
+
+def main(argv=None):
+    args = parse(argv)
     arrays, labels, _ = load_scene(args.scene, args.device)
-    if args.method == "events":
-        if args.pieces is not None:
-            parser.error("--pieces applies only to --method peel")
-        cap = EventCapacities.for_mesh(arrays[1].shape[0])
-        cap = replace(cap, **{name: getattr(cap, name) * args.pool_scale
-                              for name in ("frontier", "regions", "hits", "vertices", "triangles")})
-        p = EventPeeler(*arrays, capacities=cap, layers=args.layers)
-    else:
-        cap = Capacities.for_mesh(arrays[1].shape[0])
-        cap = replace(cap, residual=cap.residual * args.pool_scale,
-                      polygons=cap.polygons * args.pool_scale,
-                      vertices=cap.vertices * args.pool_scale,
-                      triangles=cap.triangles * args.pool_scale,
-                      pieces_per_worker=args.pieces or cap.pieces_per_worker)
-        p = DevicePeeler(*arrays, capacities=cap, layers=args.layers)
-    p.run()
-    mesh = download_mesh(p, labels)
-    info = mesh.pop("status")
+    peeler_type = METHODS[args.method][0]
+    peeler = peeler_type(*arrays, capacities=capacities(args, arrays[1].shape[0]),
+                         layers=args.layers)
+    peeler.run()
+    mesh = download_mesh(peeler, labels)
+    status = mesh.pop("status")
     args.out.parent.mkdir(parents=True, exist_ok=True)
     np.savez_compressed(args.out, **mesh)
-    args.out.with_suffix(".json").write_text(json.dumps({
-        "format": "warp-peel-approximate-v1",
-        "zero_based_layers": True,
-        "exact_geometry": False,
-        "method": args.method,
-        "scene": str(args.scene),
-        "output": info,
-    }, indent=2) + "\n")
-    print(json.dumps(info))
+    args.out.with_suffix(".json").write_text(json.dumps(sidecar(args, status), indent=2) + "\n")
+    print(json.dumps(status))
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    raise SystemExit(main())

@@ -23,6 +23,8 @@ from pathlib import Path
 
 import numpy as np
 
+from . import scenefile
+
 SCOPE = ("Sampled source-labelled ranks using independent rational ray/triangle tests, "
          "padded floating input bounds, and downloaded output polygons; not a region "
          "certificate. Grid plus output interior samples; boundary-near samples skipped.")
@@ -45,7 +47,7 @@ class RationalScene:
     binary64 bounds of their projections (audit_gpu.py:32-68)."""
 
     def __init__(self, data):
-        q = lambda x: Q(str(x))
+        q = scenefile.exact
         cam = data.get("camera", {})
         matrix = [[q(x) for x in row] for row in cam.get(
             "world_to_camera", [[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0]])]

@@ -39,37 +39,18 @@ from fractions import Fraction as Q
 
 import numpy as np
 
+from . import scenefile
 
-class ResolveError(ValueError):
-    pass
+
+# Errors in the input scene, its numbers included (the scene reader's error).
+ResolveError = scenefile.SceneFormatError
 
 
 # ---------------------------------------------------------------- numbers
 
-
-def rational(x):
-    """A scene number as an exact rational: JSON numbers exactly, strings as
-    integers or "numerator/denominator" only (src/exact_geometry.cpp:5-39)."""
-    if isinstance(x, bool):
-        raise ResolveError(f"Expected a number: {x!r}")
-    if isinstance(x, float):
-        if not np.isfinite(x):
-            raise ResolveError("Nonfinite coordinate")
-        return Q(x)
-    if isinstance(x, int):
-        return Q(x)
-    s = str(x)
-    num, _, den = s.partition("/")
-
-    def integer(v):
-        body = v[1:] if v[:1] in "+-" else v
-        return body.isdigit() and body.isascii()
-
-    if not integer(num) or (den and not integer(den)) or (_ and not den):
-        raise ResolveError(f"Expected integer or rational string: {s}")
-    if den and int(den) == 0:
-        raise ResolveError("Zero rational denominator")
-    return Q(int(num), int(den) if den else 1)
+# A scene number as an exact rational: JSON numbers exactly, strings as
+# integers or "numerator/denominator" only (src/exact_geometry.cpp:5-39).
+rational = scenefile.rational
 
 
 def text(q):
