@@ -32,6 +32,7 @@ METRIC = "device ms/mesh for all-layer peel at 64K & 720K faces, ranks exact vs 
 UNIT = "ms/mesh"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+REFERENCE_BUDGET_S = 60.0  # CPU seconds of timed extractions in the reference arm
 
 
 DESCRIPTIONS = {
@@ -156,24 +157,32 @@ def ncu_traffic(config, kernel="k_mesh_polygons"):
     return None
 
 
-def cpu_baseline(arrays, budget_s=25.0):
+def cpu_baseline(arrays, config, budget_s=25.0):
     """The reference's CPU path (fast-bvh-peel, restated) on all host threads;
-    a bounded sample: one warm-up extraction plus as many timed ones as fit."""
+    a bounded sample: one warm-up extraction plus as many timed ones as fit
+    in `budget_s` (at most 4); an extraction longer than the budget is timed
+    once, without a warm-up."""
     from oracle import fastpeel
 
     vertices, faces, camera, settings = arrays
     threads = fastpeel.max_threads()
     first, info = fastpeel.run(vertices, faces, camera, settings, threads=threads, repeat=1)
-    extra = max(1, min(4, int(budget_s / max(first[0], 1e-3))))
-    times, info = fastpeel.run(vertices, faces, camera, settings, threads=threads, repeat=extra)
+    if first[0] > budget_s:
+        times, warm = first, 0
+    else:
+        warm = 1
+        extra = max(1, min(4, int(budget_s / max(first[0], 1e-3))))
+        times, info = fastpeel.run(vertices, faces, camera, settings, threads=threads,
+                                   repeat=extra)
     return {
         "value": 1000.0 * statistics.median(times),
         "unit": UNIT,
         "cores": threads,
         "kind": "port",
-        "sample": f"full extraction of the same mesh, 1 warm-up + {extra} timed, median; "
-                  f"{info['layers']} layers, {info['triangles']} triangles; excludes import "
-                  "and projection like the reference's algorithm_seconds",
+        "sample": f"{config}: full extraction of the same mesh, {warm} warm-up + "
+                  f"{len(times)} timed, median; {info['layers']} layers, "
+                  f"{info['triangles']} triangles; excludes import and projection like the "
+                  "reference's algorithm_seconds",
     }
 
 
@@ -199,10 +208,11 @@ def run_reference(args, rank, world):
         vertices, faces = arrays[0][0], arrays[0][1]
     else:
         vertices, faces, camera, settings = arrays
-        fastpeel.run(vertices, faces, camera, settings, threads=threads,
-                     repeat=max(1, args.warmup))
+        first, _ = fastpeel.run(vertices, faces, camera, settings, threads=threads, repeat=1)
+        # Bounded: as many of the K steps as fit in REFERENCE_BUDGET_S of CPU time.
+        timed = max(1, min(args.steps, int(REFERENCE_BUDGET_S / max(first[0], 1e-3))))
         times, info = fastpeel.run(vertices, faces, camera, settings, threads=threads,
-                                   repeat=args.steps)
+                                   repeat=timed)
         ms = 1000.0 * sum(times) / len(times)
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -210,11 +220,22 @@ def run_reference(args, rank, world):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.config, vertices, faces), "impl": "reference",
         "cpu_baseline": {"value": ms, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full extractions after {max(1, args.warmup)} "
-                                   f"warm-up; {info['layers']} layers, {info['triangles']} "
-                                   "triangles"},
+                         "sample": f"{len(times)} of the {args.steps} steps timed (at most "
+                                   f"{REFERENCE_BUDGET_S:.0f} s of extractions) after 1 "
+                                   f"warm-up, mean; each a full extraction, {info['layers']} "
+                                   f"layers, {info['triangles']} triangles"},
         "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.config == "knot-65536":
+        second = scenes.CONFIGS[SECOND_CONFIG]()
+        t, info = fastpeel.run(*second, threads=threads, repeat=1)
+        line["configs"] = {SECOND_CONFIG: {
+            "value": 1000.0 * t[0], "unit": UNIT,
+            "config": workload_config(SECOND_CONFIG, second[0], second[1]),
+            "cpu_baseline": {"value": 1000.0 * t[0], "unit": UNIT, "cores": threads,
+                             "kind": "port", "sample": f"1 full extraction, no warm-up; "
+                                                       f"{info['layers']} layers, "
+                                                       f"{info['triangles']} triangles"}}}
     print(json.dumps(line), flush=True)
 
 
@@ -334,7 +355,17 @@ def run_batched(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
+def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_leg,
+                   audit_samples):
+    """Time one single-mesh configuration; returns its measurement dict.
+
+    Device time: `steps` replays of the captured extraction after
+    args.warmup, each after a 256 MiB L2 flush, CUDA events on the workspace
+    stream, max over ranks.  Stages: the graph's own per-stage timing events
+    (edp_stage_times), median over further replays.  End to end: inputs
+    uploaded from pinned host memory, the replay, status and every triangle
+    read back, per step."""
+    import numpy as np
     import torch
     import torch.distributed as dist
 
@@ -343,7 +374,7 @@ def run_ours(args, rank, world, local_rank):
 
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
-    host = scenes.CONFIGS[args.config]()
+    host = scenes.CONFIGS[config]()
     vertices, faces, camera, settings = host
     arrays = scenes.to_device(host, device)
     p, capacities = fit_event_capacities(arrays)
@@ -352,17 +383,15 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
     for _ in range(args.warmup):
         p.run()
-    info = p.read_status()
+    p.read_status()
     stream = p.stream
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    import numpy as np
-
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clocks:
-        for k in range(args.steps):
+        for k in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 starts[k].record(stream)
@@ -373,38 +402,25 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     total = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     total = max_over_ranks(total, world, device)
-    ms_per_mesh = whole_job_ms_per_mesh(total, args.steps, world)
+    ms_per_mesh = whole_job_ms_per_mesh(total, steps, world)
     check = p.read_status()
-    # Stage timing, as the reference profiles (scripts/profile_events.py): each
-    # stage replayed alone from its own captured graph, CUDA events on the
-    # workspace stream, L2 flushed before each replay.
-    stage_ms = {}
-    # Emission first: preparation resets the counters the later stages read.
-    for stage, name in ((2, "mesh_emit"), (1, "mesh_index"), (0, "prepare")):
-        times = []
-        for k in range(max(3, args.steps)):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-            _lib.check(lib.edp_run_stage(p._ws.handle, stage), "stage")
-            b.record(stream)
-            b.synchronize()
-            if k > 0:
-                times.append(a.elapsed_time(b))
-        stage_ms[name] = statistics.median(times)
-    p.run()  # restore the full extraction's state after the stage replays
-    p.read_status()
-    stage_ms["subdivision_and_rank"] = total / args.steps - sum(stage_ms.values())
 
-    # End to end through the public API: pinned host inputs uploaded each step,
-    # the extraction replayed, then status and every triangle read back.
+    # Per-stage device time from the graph's own timing events: each replay
+    # records the end of every stage, so the stages sum to the replay.
+    samples = {}
+    for _ in range(max(5, min(steps, 21))):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        p.run()
+        for name, ms in p.stage_times().items():
+            samples.setdefault(name, []).append(ms)
+    stage_ms = {name: statistics.median(v) for name, v in samples.items()}
+
     pinned = [torch.as_tensor(a).pin_memory() for a in host]
     t_count = check["triangles"]
     d2h = {name: torch.empty(tuple(getattr(p, name)[:t_count].shape),
                              dtype=getattr(p, name).dtype).pin_memory()
            for name in ("triangles_uv", "triangles_world", "triangle_sources", "triangle_layers")}
-    e2e_steps = 0 if args.quick else max(1, min(args.steps, 5))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -422,12 +438,16 @@ def run_ours(args, rank, world, local_rank):
     h2d = sum(a.numel() * a.element_size() for a in pinned)
     d2h_bytes = 64 + 152 + 128 * t_count
 
+    outside = np.zeros(2, dtype=np.int64)
+    _lib.check(lib.edp_graph_kernels(p._ws.handle, outside.ctypes.data, outside.ctypes.data + 8),
+               "graph kernels")
+    launches = int(outside[0] + outside[1] * check["rounds"])
     if rank != 0:
-        return
+        return None
     peak, peak_kind = hbm_peak()
     mesh_bytes = algorithmic_bytes(len(vertices), len(faces), check["triangles"])
-    # Noding / emission kernel: every output triangle written once (128 B), each
-    # boundary vertex read once (16 B) and each polygon's header (32 B).
+    # Noding / emission kernels: every output triangle written once (128 B),
+    # each boundary vertex read once (16 B) and each polygon's header (32 B).
     emit_bytes = 128 * check["triangles"] + 16 * check["boundary_vertices"] + 32 * check["polygons"]
     emit_ms = float(stage_ms["mesh_emit"])
     roofline = {
@@ -435,44 +455,75 @@ def run_ours(args, rank, world, local_rank):
         "kernel": "k_mesh_polygons + k_mesh_heavy (noding, fan emission, world lift)",
         "achieved": emit_bytes / (emit_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
         "frac": emit_bytes / (emit_ms * 1e-3) / 1e9 / peak,
-        "traffic": ncu_traffic(args.config),
-        "traffic_source": f"ncu capture recorded in profiles/k_mesh_polygons_{args.config}.md",
+        "traffic": ncu_traffic(config),
+        "traffic_source": f"ncu capture recorded in profiles/k_mesh_polygons_{config}.md",
         "peak_source": f"{peak_kind} copy bandwidth", "algorithmic_bytes": emit_bytes,
         "launch_ms": emit_ms,
         "pipeline": {"bytes_per_mesh": mesh_bytes,
-                     "achieved_gbs": mesh_bytes / (ms_per_mesh * 1e-3) / 1e9},
+                     "achieved_gbs": mesh_bytes / (ms_per_mesh * 1e-3) / 1e9,
+                     "frac": mesh_bytes / (ms_per_mesh * 1e-3) / 1e9 / peak},
     }
-    cpu = cpu_baseline(host) if world == 1 and not args.quick else None
-    line = {
-        "metric": METRIC, "value": ms_per_mesh, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(args.config, vertices, faces),
-        "roofline": roofline, "cpu_baseline": cpu,
+    result = {
+        "value": ms_per_mesh, "ms_per_step": total / steps, "steps": steps,
+        "config": workload_config(config, vertices, faces),
+        "roofline": roofline,
+        "cpu_baseline": cpu_baseline(host, config) if cpu_leg else None,
         "e2e": {"value": e2e_ms if e2e_steps else None, "unit": UNIT,
-                "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h_bytes)},
-        "gpu_launches": None, "clocks": clocks.summary(),
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h_bytes)},
+        "gpu_launches": int(steps * launches),
+        "kernels_per_replay": {"outside_loop": int(outside[0]), "per_round": int(outside[1]),
+                               "rounds": check["rounds"]},
+        "clocks": clocks.summary(),
         "stages_ms": stage_ms,
+        "stages_sum_ms": sum(stage_ms.values()),
         "output": {k: check[k] for k in ("polygons", "triangles", "layers", "boundary_vertices")},
         "throughput": {"fragments_per_s": check["polygons"] / (ms_per_mesh * 1e-3),
                        "triangles_per_s": check["triangles"] / (ms_per_mesh * 1e-3)},
         "capacities": vars(capacities),
     }
-    outside = np.zeros(2, dtype=np.int64)
-    _lib.check(lib.edp_graph_kernels(p._ws.handle, outside.ctypes.data, outside.ctypes.data + 8),
-               "graph kernels")
-    # Every replay launches the graph's kernel nodes, the loop body once per round.
-    line["gpu_launches"] = int(args.steps * (outside[0] + outside[1] * check["rounds"]))
-    line["kernels_per_replay"] = {"outside_loop": int(outside[0]), "per_round": int(outside[1]),
-                                  "rounds": check["rounds"]}
+    if audit_samples:
+        from peel_b200.audit import peeler_vertex_audit
+
+        report = peeler_vertex_audit(p, samples=audit_samples)
+        result["vertex_error"] = {k: report[k] for k in (
+            "polygons", "vertices_measured", "unexplained_vertices", "max_abs_error",
+            "scene_extent", "max_rel_error")}
+        result["vertex_error_max"] = report["max_rel_error"]
+    return result
+
+
+SECOND_CONFIG = "primitives-720k"  # the metric's other mesh (720K faces)
+
+
+def run_ours(args, rank, world, local_rank):
+    quick = args.quick
+    first = measure_config(args.config, args, rank, world, local_rank, args.steps,
+                          0 if quick else max(1, min(args.steps, 5)),
+                          world == 1 and not quick, 0 if quick else 400)
+    extra = {}
+    if args.config == "knot-65536" and not quick:
+        second = measure_config(SECOND_CONFIG, args, rank, world, local_rank,
+                                max(5, args.steps // 5), 3, world == 1, 300)
+        if second is not None:
+            extra[SECOND_CONFIG] = second
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": first["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": first["ms_per_step"],
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+    }
+    line.update({k: v for k, v in first.items() if k not in ("value", "ms_per_step", "steps")})
+    if extra:
+        line["configs"] = extra
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="knot-65536")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")

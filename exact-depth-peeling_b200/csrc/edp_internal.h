@@ -13,6 +13,10 @@ namespace edp {
     if (err__ != cudaSuccess) return err__;              \
   } while (0)
 
+// Records a failed CUDA call (its code and "file:line") for edp_last_cuda_error
+// and edp_last_error_site on this host thread; returns EDP_ERR_CUDA.
+int record_cuda_failure(cudaError_t e, const char *site);
+
 constexpr int kSortBlock = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortBlock * kSortItems;  // keys per radix tile
@@ -284,4 +288,13 @@ namespace edp {
 // calls note_launch), used to report how many kernels a captured graph runs.
 void note_launch();
 int64_t launch_count();
+
+// Stage marks.  While a workspace captures its own graph, `events` holds
+// EDP_STAGE_COUNT + 1 timing events; stage_mark(-1, st) records the start
+// (event 0) and stage_mark(k, st) the end of every stage up to k not yet
+// marked (a skipped stage gets a zero-length interval), as external event
+// nodes of the graph.  With no events set (eager runs, other captures) it
+// does nothing.
+void set_stage_marks(cudaEvent_t *events);
+cudaError_t stage_mark(int stage, cudaStream_t st);
 }  // namespace edp

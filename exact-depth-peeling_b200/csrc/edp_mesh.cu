@@ -2,6 +2,7 @@
 // grid (or, for very deep scenes, the layered point hierarchy), per-polygon
 // noding, centroid-fan triangulation and world lifting
 // (warp_peel/kernels.py:941-1204, events.py:720-780).
+#include "../../include/edp.h"
 #include "edp_internal.h"
 
 namespace edp {
@@ -592,12 +593,14 @@ cudaError_t stage_mesh_index(const Dev &d, SortScratch &s, TreeBuffers &point_tr
   note_launch();
   k_unique_points<<<blocks(E), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_MESH_VERTICES, st));
   EDP_CHECK(scan_exclusive(d.cell_count, d.cell_start, d.sc + kGridCells, cells, nullptr, s, st));
   k_grid_scatter<<<blocks(E), kBlock, 0, st>>>(d);
   note_launch();
   k_tree_points<<<1, 1, 0, st>>>(d);
   note_launch();
   EDP_CHECK(tree_build(point_tree, d.pt_lo, d.pt_hi, d.sc + kTreePoints, 0, true, s, st));
+  EDP_CHECK(stage_mark(EDP_STAGE_MESH_INDEX, st));
   return cudaGetLastError();
 }
 
@@ -608,6 +611,7 @@ cudaError_t stage_mesh_emit(const Dev &d, cudaStream_t st) {
   note_launch();
   k_mesh_heavy<<<148 * 5, kBlock, 0, st>>>(d, cap);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_MESH_EMIT, st));
   return cudaGetLastError();
 }
 

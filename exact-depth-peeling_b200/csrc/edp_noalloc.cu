@@ -2,13 +2,14 @@
 //
 // The workspace path (edp_event_create / edp_device_create) allocates its pools
 // with cudaMalloc when it is created.  Some callers cannot do that at the
-// point where they need welded ids: code that is recording a CUDA graph
-// (cudaMalloc is not capturable), code that runs under a caching or arena
-// allocator that owns all device memory, and real-time loops that forbid any
-// allocation after start-up.  edp_weld_noalloc gives them the welding step on
-// its own: the caller passes the vertex buffer and the output buffer, and the
-// hash-table scratch lives in a fixed array below that every GPU loading this
-// library holds until the process exits.
+// point where they need welded ids: a plugin whose host framework owns every
+// byte of device memory through its own arena or caching allocator (a raw
+// cudaMalloc there fails or fragments the arena), and real-time or serving
+// loops that forbid any allocation after start-up because an allocation can
+// block on the driver and break their latency budget.  edp_weld_noalloc gives
+// them the welding step on its own: the caller passes the vertex buffer and
+// the output buffer, and the hash-table scratch lives in a fixed array below
+// that every GPU loading this library holds until the process exits.
 #include <climits>
 #include <mutex>
 
@@ -30,12 +31,12 @@ struct WeldScratch {
 // 5 MiB per device; shared by every call on that device.
 static __device__ __align__(256) WeldScratch g_weld_scratch;
 
-struct DeviceScratch {
-  std::once_flag once;
-  WeldScratch *ptr = nullptr;
-  cudaError_t error = cudaSuccess;
-};
-DeviceScratch g_devices[kMaxDevices];
+// Device address of g_weld_scratch per device, resolved on the first call made
+// with that device current.  Only a successful lookup is cached, so a failed
+// one (for example, a first call made inside a stream capture) is retried by
+// the next call.
+std::mutex g_scratch_mutex;
+WeldScratch *g_scratch_ptr[kMaxDevices] = {};
 
 __device__ inline uint64_t position_hash(const double *v) {
   uint64_t h = edp::mix64(edp::key_bits(v[0]));
@@ -76,31 +77,51 @@ __global__ void k_noalloc_resolve(int nv, const WeldScratch *s, int *canonical) 
 
 }  // namespace
 
+#define EDP_NOALLOC_STR2(x) #x
+#define EDP_NOALLOC_STR(x) EDP_NOALLOC_STR2(x)
+#define EDP_NOALLOC_SITE __FILE__ ":" EDP_NOALLOC_STR(__LINE__)
+
 extern "C" int edp_weld_noalloc(const double *vertices, int64_t nv, int32_t *canonical,
                                 void *stream) {
   if (nv < 0 || nv > kMaxVertices) return EDP_ERR_ARGUMENT;
   if (nv == 0) return EDP_OK;
   if (!vertices || !canonical) return EDP_ERR_ARGUMENT;
   int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return EDP_ERR_CUDA;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return edp::record_cuda_failure(e, EDP_NOALLOC_SITE);
   if (device < 0 || device >= kMaxDevices) return EDP_ERR_ARGUMENT;
   // Set-up, once per device with that device current: the symbol's name is a
   // host-side stand-in, so the kernels receive its device address instead.
-  DeviceScratch &ds = g_devices[device];
-  std::call_once(ds.once, [&ds]() {
-    void *ptr = nullptr;
-    ds.error = cudaGetSymbolAddress(&ptr, g_weld_scratch);
-    ds.ptr = static_cast<WeldScratch *>(ptr);
-  });
-  if (ds.error != cudaSuccess || !ds.ptr) return EDP_ERR_CUDA;
+  WeldScratch *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[device]) {
+      void *ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_weld_scratch);
+      if (e != cudaSuccess || !ptr)
+        return edp::record_cuda_failure(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                                        EDP_NOALLOC_SITE);
+      g_scratch_ptr[device] = static_cast<WeldScratch *>(ptr);
+    }
+    scratch = g_scratch_ptr[device];
+  }
   const int mask = int(edp::pow2_at_least(2 * nv) - 1);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned clear_blocks = unsigned(edp::ceil_div(int64_t(mask) + 1, 256) < 1184
                                              ? edp::ceil_div(int64_t(mask) + 1, 256)
                                              : 1184);
   const unsigned blocks = unsigned(edp::ceil_div(nv, 256) < 1184 ? edp::ceil_div(nv, 256) : 1184);
-  k_noalloc_clear<<<clear_blocks, 256, 0, st>>>(ds.ptr, mask);
-  k_noalloc_insert<<<blocks, 256, 0, st>>>(vertices, int(nv), ds.ptr, mask);
-  k_noalloc_resolve<<<blocks, 256, 0, st>>>(int(nv), ds.ptr, canonical);
-  return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+  // Launch errors are read without clearing the thread's error state: an
+  // error left pending by the caller's own earlier work stays pending for the
+  // caller (this call reports it too, as EDP_ERR_CUDA).
+  k_noalloc_clear<<<clear_blocks, 256, 0, st>>>(scratch, mask);
+  if ((e = cudaPeekAtLastError()) != cudaSuccess)
+    return edp::record_cuda_failure(e, EDP_NOALLOC_SITE);
+  k_noalloc_insert<<<blocks, 256, 0, st>>>(vertices, int(nv), scratch, mask);
+  if ((e = cudaPeekAtLastError()) != cudaSuccess)
+    return edp::record_cuda_failure(e, EDP_NOALLOC_SITE);
+  k_noalloc_resolve<<<blocks, 256, 0, st>>>(int(nv), scratch, canonical);
+  if ((e = cudaPeekAtLastError()) != cudaSuccess)
+    return edp::record_cuda_failure(e, EDP_NOALLOC_SITE);
+  return EDP_OK;
 }

@@ -4,6 +4,7 @@
 // (the role of the reference's conditional sort buckets, events.py:637-718).
 #include <cub/warp/warp_scan.cuh>
 
+#include "../../include/edp.h"
 #include "edp_internal.h"
 
 namespace edp {
@@ -440,7 +441,27 @@ cudaError_t tree_build(TreeBuffers &t, const float4 *lo, const float4 *hi, const
 namespace edp {
 namespace {
 thread_local int64_t g_launches = 0;
+thread_local cudaEvent_t *g_marks = nullptr;
+thread_local int g_next_mark = 0;  // stages marked so far in this capture
 }
 void note_launch() { ++g_launches; }
 int64_t launch_count() { return g_launches; }
+
+void set_stage_marks(cudaEvent_t *events) {
+  g_marks = events;
+  g_next_mark = 0;
+}
+
+cudaError_t stage_mark(int stage, cudaStream_t st) {
+  if (!g_marks) return cudaSuccess;
+  if (stage < 0) {  // the start
+    g_next_mark = 0;
+    return cudaEventRecordWithFlags(g_marks[0], st, cudaEventRecordExternal);
+  }
+  for (; g_next_mark <= stage && g_next_mark < EDP_STAGE_COUNT; ++g_next_mark) {
+    cudaError_t e = cudaEventRecordWithFlags(g_marks[g_next_mark + 1], st, cudaEventRecordExternal);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
 }  // namespace edp

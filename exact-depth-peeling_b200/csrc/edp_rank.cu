@@ -4,6 +4,7 @@
 // continuation), the per-group hit order, per-polygon rank assignment and the
 // optional convex merge (warp_peel/events.py:291-635, components.py, beams.py,
 // event_kernels.py:28-385).
+#include "../../include/edp.h"
 #include "edp_internal.h"
 
 namespace edp {
@@ -957,6 +958,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   EDP_CHECK(order_polygons(d, false, s, st));
   k_polygon_init<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_ORDER, st));
   const bool connected = d.propagate_ranks || d.merge_regions;
   if (connected) {
     EDP_CHECK(scan_exclusive(d.counts, d.offsets, d.sc + kLivePolygons, R, d.sc + kPatchEdges, s, st));
@@ -980,10 +982,12 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     }
     note_launch();
   }
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_CONNECTIVITY, st));
   k_roots<<<blocks(R), kBlock, 0, st>>>(d, d.propagate_ranks ? 1 : 0);
   note_launch();
   k_samples<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_SAMPLES, st));
   EDP_CHECK(cudaMemsetAsync(d.sample_table, 0xff, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.sample_min, 0x7f, sizeof(int) * (int64_t(d.sample_mask) + 1), st));
   k_cells_reset<<<kCells / 128, 128, 0, st>>>(d);
@@ -992,6 +996,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   note_launch();
   k_group_resolve<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_QUERY_GROUPS, st));
   if (d.share_regions) {
     k_certify<<<kCells * 32 / kBlock, kBlock, 0, st>>>(d);
     note_launch();
@@ -1000,6 +1005,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_apply_cells<<<blocks(R), kBlock, 0, st>>>(d);
     note_launch();
   }
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_CERTIFY, st));
   {
     const int64_t cells = int64_t(d.grid_size) * d.grid_size;
     EDP_CHECK(cudaMemsetAsync(d.ray_count, 0, sizeof(int) * cells, st));
@@ -1012,10 +1018,13 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_ray_grid_fill<<<blocks(d.n), kBlock, 0, st>>>(d);
     note_launch();
   }
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_GRID, st));
   k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_PRIMARY, st));
   k_heavy_hits<<<148 * 16, kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_HEAVY, st));
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
   k_check_hits<<<1, 1, 0, st>>>(d);
   note_launch();
@@ -1035,10 +1044,12 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   note_launch();
   k_group_sort<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_HIT_SORT, st));
   k_layers_reset<<<1, 1, 0, st>>>(d);
   note_launch();
   k_assign<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_ASSIGN, st));
   if (d.merge_regions) {
     EDP_CHECK(cudaMemsetAsync(d.merge_choice, 0x7f, sizeof(int) * R, st));
     k_merge_propose<<<blocks(E), kBlock, 0, st>>>(d);
@@ -1055,6 +1066,7 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     k_merge_finish<<<1, 1, 0, st>>>(d);
     note_launch();
   }
+  EDP_CHECK(stage_mark(EDP_STAGE_RANK_MERGE, st));
   return cudaGetLastError();
 }
 

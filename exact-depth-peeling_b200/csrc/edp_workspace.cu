@@ -36,6 +36,10 @@ struct edp_peeler {
   // Kernel nodes of the last capture: outside the subdivision loop, and in
   // one iteration of its body.
   int64_t kernels_outside = 0, kernels_per_round = 0;
+  // Stage timing events recorded by the workspace's own graph (start, then
+  // the end of each EDP_STAGE_*); created with the graph.
+  cudaEvent_t marks[EDP_STAGE_COUNT + 1] = {};
+  bool marked = false;
 };
 
 namespace {
@@ -43,11 +47,7 @@ namespace {
 thread_local int g_last_cuda = 0;
 thread_local const char *g_last_site = "";
 
-int cuda_fail(cudaError_t e, const char *site) {
-  g_last_cuda = int(e);
-  g_last_site = site;
-  return EDP_ERR_CUDA;
-}
+int cuda_fail(cudaError_t e, const char *site) { return edp::record_cuda_failure(e, site); }
 
 #define EDP_STR2(x) #x
 #define EDP_STR(x) EDP_STR2(x)
@@ -297,9 +297,16 @@ cudaError_t run_body(edp_peeler *p, const Dev &d, cudaStream_t st) {
                         : stage_device_layer(d, p->scratch, p->source_tree, p->residual_tree, st);
 }
 cudaError_t run_finish(edp_peeler *p, const Dev &d, cudaStream_t st) {
-  EDP_CHECK(p->method == 0 ? stage_rank(d, p->scratch, st) : stage_device_finish(d, st));
+  if (p->method == 0) {
+    EDP_CHECK(stage_rank(d, p->scratch, st));
+  } else {  // its finish is timed as the assignment stage
+    EDP_CHECK(stage_mark(EDP_STAGE_RANK_HIT_SORT, st));
+    EDP_CHECK(stage_device_finish(d, st));
+    EDP_CHECK(stage_mark(EDP_STAGE_RANK_MERGE, st));
+  }
   EDP_CHECK(stage_mesh_index(d, p->scratch, p->point_tree, st));
-  return stage_mesh_emit(d, st);
+  EDP_CHECK(stage_mesh_emit(d, st));
+  return stage_mark(EDP_STAGE_COUNT - 1, st);
 }
 
 // The whole extraction, recorded on `st`.  With `graph` the loop becomes a
@@ -331,7 +338,9 @@ int enqueue(edp_peeler *p, cudaStream_t st, bool graph) {
   d.use_handle = 1;
   d.cond_handle = handle;
   const int64_t first_launch = launch_count();
+  EDP_TRY(stage_mark(-1, st));
   EDP_TRY(run_prepare(p, d, st));
+  EDP_TRY(stage_mark(EDP_STAGE_PREPARE, st));
   EDP_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
   cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
@@ -352,6 +361,7 @@ int enqueue(edp_peeler *p, cudaStream_t st, bool graph) {
   cudaError_t end = cudaStreamEndCapture(p->body_stream, &captured);
   EDP_TRY(step);
   EDP_TRY(end);
+  EDP_TRY(stage_mark(EDP_STAGE_SUBDIVIDE, st));
   EDP_TRY(run_finish(p, d, st));
   p->kernels_per_round = per_round;
   p->kernels_outside = launch_count() - first_launch - per_round;
@@ -368,6 +378,12 @@ int check_inputs(const double *vertices, int64_t nv, const int32_t *faces, int64
 }
 
 }  // namespace
+
+int edp::record_cuda_failure(cudaError_t e, const char *site) {
+  g_last_cuda = int(e);
+  g_last_site = site;
+  return EDP_ERR_CUDA;
+}
 
 extern "C" {
 
@@ -519,8 +535,12 @@ int edp_capture(edp_peeler *p) {
     int rc = edp_warmup(p);
     if (rc) return rc;
   }
+  for (cudaEvent_t &ev : p->marks)
+    if (!ev) EDP_TRY(cudaEventCreate(&ev));
   EDP_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  set_stage_marks(p->marks);
   int rc = enqueue(p, p->stream, true);
+  set_stage_marks(nullptr);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(p->stream, &g);
   if (rc) {
@@ -529,6 +549,7 @@ int edp_capture(edp_peeler *p) {
   }
   EDP_TRY(e);
   p->graph = g;
+  p->marked = true;
   EDP_TRY(cudaGraphInstantiate(&p->exec, g, 0));
   return EDP_OK;
 }
@@ -585,6 +606,8 @@ void edp_destroy(edp_peeler *p) {
   if (p->body_stream) cudaStreamDestroy(p->body_stream);
   for (auto &e : p->stage_exec)
     if (e) cudaGraphExecDestroy(e);
+  for (cudaEvent_t ev : p->marks)
+    if (ev) cudaEventDestroy(ev);
   delete p;
 }
 
@@ -624,6 +647,15 @@ int edp_run_stage(edp_peeler *p, int32_t stage) {
     EDP_TRY(e);
   }
   EDP_TRY(cudaGraphLaunch(p->stage_exec[stage], p->stream));
+  return EDP_OK;
+}
+
+int edp_stage_times(edp_peeler *p, float *ms) {
+  if (!p || !ms) return EDP_ERR_ARGUMENT;
+  if (!p->marked) return EDP_ERR_STATE;  // no replay of the workspace's own graph yet
+  EDP_TRY(cudaEventSynchronize(p->marks[EDP_STAGE_COUNT]));
+  for (int k = 0; k < EDP_STAGE_COUNT; ++k)
+    EDP_TRY(cudaEventElapsedTime(&ms[k], p->marks[k], p->marks[k + 1]));
   return EDP_OK;
 }
 

@@ -8,7 +8,7 @@ import ctypes
 from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libedp_b200.so"
-ABI_VERSION = 2  # EDP_ABI_VERSION in include/edp.h
+ABI_VERSION = 3  # EDP_ABI_VERSION in include/edp.h
 
 I64 = ctypes.c_int64
 I32 = ctypes.c_int32
@@ -44,7 +44,15 @@ EXPORTS = (
     "edp_event_create", "edp_device_create", "edp_event_default_capacities",
     "edp_device_default_capacities", "edp_warmup", "edp_enqueue", "edp_capture", "edp_run",
     "edp_read_status", "edp_get_outputs", "edp_destroy", "edp_status_string",
-    "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels", "edp_last_error_site",
+    "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
+    "edp_last_error_site", "edp_weld_noalloc", "edp_stage_times",
+)
+
+# enum edp_stage in include/edp.h, in order (edp_stage_times fills one float each).
+STAGE_NAMES = (
+    "prepare", "subdivide", "rank_order", "rank_connectivity", "rank_samples",
+    "rank_query_groups", "rank_certify", "rank_ray_grid", "rank_ray_primary", "rank_ray_heavy",
+    "rank_hit_sort", "rank_assign", "rank_merge", "mesh_vertices", "mesh_index", "mesh_emit",
 )
 
 _lib = None
@@ -80,6 +88,9 @@ def load():
     lib.edp_get_outputs.argtypes = [P, ctypes.POINTER(OutputsC)]
     lib.edp_run_stage.argtypes = [P, I32]
     lib.edp_graph_kernels.argtypes = [P, P, P]
+    lib.edp_stage_times.argtypes = [P, P]
+    lib.edp_weld_noalloc.argtypes = [P, I64, P, P]
+    lib.edp_weld_noalloc.restype = ctypes.c_int
     lib.edp_destroy.argtypes = [P]
     lib.edp_destroy.restype = None
     lib.edp_status_string.argtypes = [ctypes.c_int]

@@ -222,6 +222,14 @@ class _Peeler:
             self.capture()
         self._ws.call("edp_run", "run")
 
+    def stage_times(self):
+        """{stage: device ms} of the last replay of this peeler's own graph
+        (run() / capture()), from timing events the graph records at each
+        stage's end; waits for that replay.  The values sum to its time."""
+        ms = np.zeros(len(_lib.STAGE_NAMES), dtype=np.float32)
+        _lib.check(_lib.load().edp_stage_times(self._ws.handle, ms.ctypes.data), "stage times")
+        return dict(zip(_lib.STAGE_NAMES, map(float, ms)))
+
 
 class DevicePeeler(_Peeler):
     """Iterative per-layer clipping (warp_peel/solver.py:92-519).

@@ -46,7 +46,7 @@ enum edp_status {
 enum {
   EDP_STATUS_SLOTS = 16,
   EDP_METRICS = 20,
-  EDP_ABI_VERSION = 2,
+  EDP_ABI_VERSION = 3,
   EDP_ERR_BIT_POLYGON = 1,
   EDP_ERR_BIT_WORKER = 2,
   EDP_ERR_BIT_RESIDUAL = 4,
@@ -136,24 +136,61 @@ void edp_destroy(edp_peeler *p);
  * captured stage graphs (scripts/profile_events.py:35-98).  Replaying stage 0
  * resets the counters, so run the full graph again before reading outputs. */
 int edp_run_stage(edp_peeler *p, int32_t stage);
+/* Stages timed by edp_stage_times, in extraction order: the reference
+ * profiler's phases (scripts/profile_events.py:35-56) with its rank and mesh
+ * phases split where this build's kernels split.  The DevicePeeler fills
+ * PREPARE, SUBDIVIDE (its layer loop), RANK_ASSIGN (its finish), and the
+ * three MESH stages; its other stages read 0. */
+enum edp_stage {
+  EDP_STAGE_PREPARE = 0,       /* validation, weld, projection, contours, hierarchies */
+  EDP_STAGE_SUBDIVIDE,         /* the subdivision (or layer) loop, all rounds */
+  EDP_STAGE_RANK_ORDER,        /* Morton order of the output polygons */
+  EDP_STAGE_RANK_CONNECTIVITY, /* patch edges, edge match, connection test */
+  EDP_STAGE_RANK_SAMPLES,      /* union-find roots and representative samples */
+  EDP_STAGE_RANK_QUERY_GROUPS, /* exact-coordinate sample groups */
+  EDP_STAGE_RANK_CERTIFY,      /* certified rectangles */
+  EDP_STAGE_RANK_RAY_GRID,     /* the source grid the rays read */
+  EDP_STAGE_RANK_RAY_PRIMARY,  /* primary ray hits */
+  EDP_STAGE_RANK_RAY_HEAVY,    /* heavy-ray continuation */
+  EDP_STAGE_RANK_HIT_SORT,     /* hit counts, scan and per-group hit order */
+  EDP_STAGE_RANK_ASSIGN,       /* layer assignment */
+  EDP_STAGE_RANK_MERGE,        /* optional convex merge */
+  EDP_STAGE_MESH_VERTICES,     /* boundary vertex scan and distinct points */
+  EDP_STAGE_MESH_INDEX,        /* point grid and point hierarchy */
+  EDP_STAGE_MESH_EMIT,         /* noding, fans, world lift */
+  EDP_STAGE_COUNT
+};
+/* Per-stage device milliseconds of the most recent replay of the workspace's
+ * own graph (edp_capture / edp_run), from timing events the graph records at
+ * each stage's end; waits for that replay.  ms receives EDP_STAGE_COUNT
+ * values, which sum to the replay's time.  No counterpart call in the
+ * reference, whose profiler captures each stage as a separate graph. */
+int edp_stage_times(edp_peeler *p, float *ms);
+
 /* Kernel nodes of the captured graph: outside the subdivision loop, and per
  * loop iteration (a replay launches outside + per_round * rounds kernels). */
 int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
 
 /* Exact-position welding without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc where they need
- * welded ids (while recording a CUDA graph, under an allocator that owns all
- * device memory, or in a loop that must not allocate after start-up).
+ * welded ids - a plugin whose host framework owns all device memory through its
+ * own arena or caching allocator, or a real-time loop that must not allocate
+ * after start-up because an allocation can block on the driver.
  * canonical[i] receives the smallest index j with vertices[j] equal to
  * vertices[i] (signed zeros equal) - the same ids as edp_get_outputs'
- * `canonical`.  Both buffers are the caller's device memory; kernels run on
- * `stream`.  The hash-table scratch is a fixed 5 MiB device array that every
- * GPU loading this library holds until the process exits, so nv is limited to
- * EDP_WELD_NOALLOC_MAX_VERTICES (larger nv returns EDP_ERR_ARGUMENT).  The
- * first call on a device resolves that array's device address; make it before
- * any stream capture.  All calls on a device share the array and each call
- * clears the part it uses first: calls that overlap on the GPU (different
- * streams, or different host threads) race and give undefined ids. */
+ * `canonical`.  Vertices must be finite: a vertex with a NaN coordinate equals
+ * no vertex, itself included, and keeps its own index (the workspace path
+ * flags such input with EDP_ERR_BIT_INPUT instead).  Both buffers are the
+ * caller's device memory; kernels run on `stream`.  The hash-table scratch is
+ * a fixed 5 MiB device array that every GPU loading this library holds until
+ * the process exits, so nv is limited to EDP_WELD_NOALLOC_MAX_VERTICES (larger
+ * nv returns EDP_ERR_ARGUMENT).  The first call on a device, made with that
+ * device current, resolves that array's device address; make it before any
+ * stream capture (a failed lookup returns EDP_ERR_CUDA and is retried by the
+ * next call).  All calls on a device share the array, which keeps the last
+ * call's contents; each call clears the part it uses first.  Calls that
+ * overlap on the GPU (different streams, or different host threads) race and
+ * give undefined ids. */
 #define EDP_WELD_NOALLOC_MAX_VERTICES 262144
 int edp_weld_noalloc(const double *vertices, int64_t nv, int32_t *canonical, void *stream);
 
@@ -162,8 +199,8 @@ const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
 /* Source location ("file:line") of the CUDA call behind the last EDP_ERR_CUDA. */
 const char *edp_last_error_site(void);
-/* EDP_ABI_VERSION of the library: 2 since metrics[] holds 20 counters
- * (heavy_noded_polygons added); 1 had 19. */
+/* EDP_ABI_VERSION of the library: 3 since edp_stage_times; 2 had metrics[]
+ * of 20 counters (heavy_noded_polygons added); 1 had 19. */
 int edp_abi_version(void);
 
 #ifdef __cplusplus

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     for name in declared():
         assert hasattr(lib, name), name
-    assert set(declared()) <= set(_lib.EXPORTS) | {"edp_weld_noalloc"}
+    assert set(declared()) <= set(_lib.EXPORTS)
     assert lib.edp_abi_version() >= 1
     assert lib.edp_status_string(1) == b"invalid argument"
 
@@ -88,3 +88,13 @@ def test_host_inputs_are_validated():
     with pytest.raises(ValueError):
         EventPeeler(torch.zeros((3, 3), dtype=torch.float64), torch.zeros((1, 3), dtype=torch.int32),
                     torch.eye(4, dtype=torch.float64), torch.zeros(6, dtype=torch.float64))
+
+
+def test_stage_names_match_the_header():
+    """The Python stage names follow enum edp_stage, one per value."""
+    from peel_b200 import _lib
+
+    text = (ROOT / "include/edp.h").read_text()
+    body = text[text.index("enum edp_stage {"):text.index("EDP_STAGE_COUNT\n")]
+    names = re.findall(r"EDP_STAGE_([A-Z_]+)", body)
+    assert [n.lower() for n in names] == list(_lib.STAGE_NAMES)
