@@ -355,8 +355,26 @@ def run_batched(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def time_replays(p, steps, flush):
+    """Mean device ms of `steps` replays of p's graph, each after an L2 flush
+    (CUDA events on the workspace stream)."""
+    import torch
+
+    total = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(p.stream):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(p.stream)
+        p.run()
+        b.record(p.stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total / max(steps, 1)
+
+
 def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_leg,
-                   audit_samples):
+                   audit_samples, compare_forms=False):
     """Time one single-mesh configuration; returns its measurement dict.
 
     Device time: `steps` replays of the captured extraction after
@@ -489,6 +507,32 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
             "polygons", "vertices_measured", "unexplained_vertices", "max_abs_error",
             "scene_extent", "max_rel_error")}
         result["vertex_error_max"] = report["max_rel_error"]
+    if compare_forms:
+        # The same extraction with the reference's plain binary64 predicates
+        # (the comparator of the filtered form), and one counted extraction
+        # for the filters' escalation rates.
+        del p
+        plain, _ = fit_event_capacities(arrays, capacities, predicates="binary64")
+        plain.capture()
+        for _ in range(args.warmup):
+            plain.run()
+        plain_ms = time_replays(plain, steps, flush)
+        plain_info = plain.read_status()
+        del plain
+        counted, _ = fit_event_capacities(arrays, capacities, predicates="counted")
+        counted.run()
+        counts = counted.predicate_counts()
+        del counted
+        result["predicates"] = {
+            "form": "filtered",
+            "filtered_ms": ms_per_mesh, "binary64_ms": plain_ms,
+            "binary64_over_filtered": plain_ms / ms_per_mesh,
+            "binary64_output": {k: plain_info[k] for k in ("polygons", "triangles", "layers")},
+            "counts": counts,
+            "escalated_share": {c: (v["binary64"] + v["exact"]) / max(1, sum(v.values()))
+                                for c, v in counts.items()},
+            "exact_share": {c: v["exact"] / max(1, sum(v.values())) for c, v in counts.items()},
+        }
     return result
 
 
@@ -499,11 +543,13 @@ def run_ours(args, rank, world, local_rank):
     quick = args.quick
     first = measure_config(args.config, args, rank, world, local_rank, args.steps,
                           0 if quick else max(1, min(args.steps, 5)),
-                          world == 1 and not quick, 0 if quick else 400)
+                          world == 1 and not quick, 0 if quick else 400,
+                          compare_forms=not quick)
     extra = {}
     if args.config == "knot-65536" and not quick:
         second = measure_config(SECOND_CONFIG, args, rank, world, local_rank,
-                                max(5, args.steps // 5), 3, world == 1, 300)
+                                max(5, args.steps // 5), 3, world == 1, 300,
+                                compare_forms=True)
         if second is not None:
             extra[SECOND_CONFIG] = second
     if rank != 0:

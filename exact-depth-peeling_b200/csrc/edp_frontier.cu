@@ -1,5 +1,6 @@
 // Contour-guided convex subdivision: one round of the device-controlled loop
 // (warp_peel/frontier.py:81-245, event_kernels.py:12-25).
+#include "edp_filtered.cuh"
 #include "edp_internal.h"
 
 namespace edp {
@@ -69,9 +70,20 @@ struct Segments {
   const V2 *a, *b, *near;
 };
 
-// First cutting lane of a batch, or -1; a, b are its segment.
+// Predicate tallies of one subdivision warp (counted form only).
+struct CutTally {
+  Tally side, segment, depth;
+};
+
+// First cutting lane of a batch, or -1; a, b are its segment and `side` this
+// lane's vertex against its line (the split reuses it).  F is the predicate
+// form (edp_filtered.cuh): the plain form evaluates the reference's binary64
+// expressions; the filtered forms take exact signs of the sides, of the
+// segment ends against the patch edges and of the depth differences, and
+// keep binary64 for the clip parameters.
+template <int F>
 __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 q, int n,
-                                const Plane &sc, V2 &a, V2 &b) {
+                                const Plane &sc, V2 &a, V2 &b, int &side, CutTally &tally) {
   const int lane = threadIdx.x & 31;
   const bool mine = lane < n;
   const int width = lane_width(n);
@@ -87,26 +99,73 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
     batch &= batch - 1;
     a = shfl(ca, k);
     b = shfl(cb, k);
-    const double side = cross(a, b, p);
-    if (!__ballot_sync(kFull, mine && side > 0.0) || !__ballot_sync(kFull, mine && side < 0.0))
+    int stage = 0;
+    if constexpr (F == 0) {
+      side = sign_of(cross(a, b, p));
+    } else {
+      side = mine ? side_sign<F>(a, b, p, stage) : 0;
+      if constexpr (F == 2)
+        if (mine) tally.side.add(stage);
+    }
+    if (!__ballot_sync(kFull, mine && side > 0) || !__ballot_sync(kFull, mine && side < 0))
       continue;
     const V2 near = shfl(cn, k);
     const double za = value(sc, a) - near.x, zb = value(sc, b) - near.y;
-    if (za <= 0.0 && zb <= 0.0) continue;
+    int sza, szb;
+    if constexpr (F == 0) {
+      sza = sign_of(za);
+      szb = sign_of(zb);
+    } else {
+      int stage_b = 0;
+      sza = plane_sign<F>(sc, a, near.x, stage);
+      szb = plane_sign<F>(sc, b, near.y, stage_b);
+      if constexpr (F == 2) {
+        if (lane == 0) {  // the same test on every lane: count it once
+          tally.depth.add(stage);
+          tally.depth.add(stage_b);
+        }
+      }
+    }
+    if (sza <= 0 && szb <= 0) continue;
     const double da = cross(p, q, a), db = cross(p, q, b);
-    if (__ballot_sync(kFull, mine && da <= 0.0 && db <= 0.0)) continue;
-    const double r = da / (da - db);
-    double low = mine && da < 0.0 ? fmax(0.0, r) : 0.0;
-    double high = mine && db < 0.0 ? fmin(1.0, r) : 1.0;
+    int sda, sdb;
+    if constexpr (F == 0) {
+      sda = sign_of(da);
+      sdb = sign_of(db);
+    } else {
+      int stage_b = 0;
+      sda = mine ? side_sign<F>(p, q, a, stage) : 0;
+      sdb = mine ? side_sign<F>(p, q, b, stage_b) : 0;
+      if constexpr (F == 2) {
+        if (mine) {
+          tally.segment.add(stage);
+          tally.segment.add(stage_b);
+        }
+      }
+    }
+    if (__ballot_sync(kFull, mine && sda <= 0 && sdb <= 0)) continue;
+    double low, high, rz;
+    if constexpr (F == 0) {
+      const double r = da / (da - db);
+      low = mine && da < 0.0 ? fmax(0.0, r) : 0.0;
+      high = mine && db < 0.0 ? fmin(1.0, r) : 1.0;
+    } else {
+      const double r = crossing(da, db);
+      low = mine && sda < 0 ? r : 0.0;
+      high = mine && sdb < 0 ? r : 1.0;
+    }
     for (int off = width >> 1; off > 0; off >>= 1) {  // lanes [0, width) hold the edges
       low = fmax(low, __shfl_xor_sync(kFull, low, off));
       high = fmin(high, __shfl_xor_sync(kFull, high, off));
     }
     low = __shfl_sync(kFull, low, 0);
     high = __shfl_sync(kFull, high, 0);
-    const double rz = za / (za - zb);
-    if (za < 0.0) low = fmax(low, rz);
-    if (zb < 0.0) high = fmin(high, rz);
+    if constexpr (F == 0)
+      rz = za / (za - zb);
+    else
+      rz = crossing(za, zb);
+    if (sza < 0) low = fmax(low, rz);
+    if (szb < 0) high = fmin(high, rz);
     if (high > low) return k;
   }
   return -1;
@@ -156,8 +215,11 @@ __device__ inline int warp_clean(V2 &x, int m, V2 *buf) {
 // both cleaned: the vertex sequence of the sequential split (kernels.py:184-203)
 // placed with ballots and prefix counts.  Returns false when a part exceeds
 // kMaxVertices.
-__device__ inline bool warp_split(V2 p, V2 q, int n, V2 a, V2 b, V2 *left, V2 *right, V2 &pl,
-                                  int &nl, V2 &pr, int &nr) {
+// The filtered forms (F > 0) classify the vertices by `side`, the exact sign
+// first_cut found, and place the cut points with the binary64 values.
+template <int F>
+__device__ inline bool warp_split(V2 p, V2 q, int n, V2 a, V2 b, int side, V2 *left, V2 *right,
+                                  V2 &pl, int &nl, V2 &pr, int &nr) {
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const V2 dir = b - a;
@@ -165,8 +227,17 @@ __device__ inline bool warp_split(V2 p, V2 q, int n, V2 a, V2 b, V2 *left, V2 *r
   const bool mine = lane < n;
   const double du = value(s, p - a);
   const double dv = __shfl_sync(kFull, du, lane + 1 < n ? lane + 1 : 0);
-  const bool in = mine && du >= 0.0, out = mine && du <= 0.0;
-  const bool cut = mine && ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0));
+  bool in, out, cut;
+  if constexpr (F == 0) {
+    in = mine && du >= 0.0;
+    out = mine && du <= 0.0;
+    cut = mine && ((du > 0.0 && dv < 0.0) || (du < 0.0 && dv > 0.0));
+  } else {
+    const int sv = __shfl_sync(kFull, side, lane + 1 < n ? lane + 1 : 0);
+    in = mine && side >= 0;
+    out = mine && side <= 0;
+    cut = mine && ((side > 0 && sv < 0) || (side < 0 && sv > 0));
+  }
   const unsigned bin = __ballot_sync(kFull, in), bout = __ballot_sync(kFull, out);
   const unsigned bcut = __ballot_sync(kFull, cut);
   nl = __popc(bin) + __popc(bcut);
@@ -177,7 +248,7 @@ __device__ inline bool warp_split(V2 p, V2 q, int n, V2 a, V2 b, V2 *left, V2 *r
   if (in) left[at_l] = p;
   if (out) right[at_r] = p;
   if (cut) {
-    const V2 x = p + (du / (du - dv)) * (q - p);
+    const V2 x = p + (F == 0 ? du / (du - dv) : crossing(du, dv)) * (q - p);
     left[at_l + (in ? 1 : 0)] = x;
     right[at_r + (out ? 1 : 0)] = x;
   }
@@ -228,6 +299,7 @@ __device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int
 // tested against the part's box when they are expanded.  A patch that has
 // met every candidate is final and goes to the output pool; one that spends
 // its budget carries over.  Warps take patches from a shared counter.
+template <int F>
 __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
   __shared__ V2 s_parts[kWarps][2][kMaxVertices];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -242,6 +314,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
   const Frontier next{d.fv[par ^ 1], d.fn[par ^ 1], d.fsrc[par ^ 1], d.fcur[par ^ 1],
                       &d.status[kNextResidual], d.status, d.cap.frontier};
   long long visits = 0, tests = 0, splits = 0;  // lane 0's tallies
+  CutTally tally;
   for (;;) {
     int i = 0, failed = 0;
     if (lane == 0) {
@@ -266,10 +339,10 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
     walk_begin(w, d.seg_tree, leaves, lo, hi, cursor);
     for (;;) {
       unsigned batch;
-      int first, resume = leaves, cut = -1;
+      int first, resume = leaves, cut = -1, side = 0;
       V2 a, b;
       while (walk_next(w, d.seg_tree, leaves, lo, hi, cursor, budget, batch, first, resume)) {
-        cut = first_cut(segs, batch, first, p, q, n, sc, a, b);
+        cut = first_cut<F>(segs, batch, first, p, q, n, sc, a, b, side, tally);
         tests += __popc(cut >= 0 ? batch & (kFull >> (31 - cut)) : batch);  // met up to the cut
         if (cut >= 0) break;
       }
@@ -296,7 +369,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
       cursor = first + cut + 1;
       V2 pl, pr;
       int nl, nr;
-      if (!warp_split(p, q, n, a, b, left_part, right_part, pl, nl, pr, nr)) {
+      if (!warp_split<F>(p, q, n, a, b, side, left_part, right_part, pl, nl, pr, nr)) {
         if (lane == 0) set_error(d.status, kErrPolygon);
         break;
       }
@@ -317,6 +390,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
     count_add(&d.metrics[kTargetVisits], visits);
     count_add(&d.metrics[kContourTests], tests);
     count_add(&d.metrics[kSplits], splits);
+  }
+  if constexpr (F == 2) {
+    tally.side.flush(d, kPredSide);
+    tally.segment.flush(d, kPredSegment);
+    tally.depth.flush(d, kPredDepth);
   }
 }
 
@@ -340,7 +418,7 @@ __global__ void k_advance(Dev d) {
 cudaError_t stage_step(const Dev &d, cudaStream_t st) {
   int64_t g = ceil_div(d.cap.frontier, kWarps);
   if (g > 148 * 8) g = 148 * 8;
-  k_subdivide<<<unsigned(g), kBlock, 0, st>>>(d);
+  EDP_LAUNCH_FORM(d.predicates, k_subdivide, unsigned(g), kBlock, st, d);
   note_launch();
   k_advance<<<1, 1, 0, st>>>(d);
   note_launch();

@@ -118,6 +118,9 @@ enum Scalar : int {
   kScalarCount = 24
 };
 
+// Predicate tallies: six classes by three deciding stages (edp_filtered.cuh).
+constexpr int kPredCounters = 18;
+
 // Every device pointer of a workspace, passed by value to the kernels.
 struct Dev {
   const double *vertices;
@@ -126,6 +129,10 @@ struct Dev {
   const double *settings;
   int nv, n;
   int limit, all_layers, share_regions, propagate_ranks, merge_regions;
+  // Sign predicates: 0 plain binary64, 1 filtered exact, 2 filtered exact
+  // and counted into pred_counts ([class][stage], edp_filtered.cuh).
+  int predicates;
+  unsigned long long *pred_counts;
   Caps cap;
 
   int *status;

@@ -16,6 +16,7 @@ __global__ void k_reset(Dev d) {
   if (i < kStatusSlots) d.status[i] = 0;
   if (i < kMetrics) d.metrics[i] = 0;
   if (i < kScalarCount) d.sc[i] = 0;
+  if (i < kPredCounters) d.pred_counts[i] = 0;
   if (i == 0) {
     d.sc[kSourceCount] = d.n;
     d.sc[kSegmentSlots] = kSourceVertices * d.n;

@@ -5,6 +5,7 @@
 // optional convex merge (warp_peel/events.py:291-635, components.py, beams.py,
 // event_kernels.py:28-385).
 #include "../../include/edp.h"
+#include "edp_filtered.cuh"
 #include "edp_internal.h"
 
 namespace edp {
@@ -481,14 +482,19 @@ __global__ void k_apply_cells(Dev d) {
 // Half-open containment: a point on an edge belongs to the polygon only if the
 // edge is "owned" (rising, or horizontal running in -x), so a tessellated
 // sheet counts once on shared edges (event_kernels.py:95-148).
-__device__ inline bool contains_flat(const Dev &d, int source, V2 x) {
+// F is the predicate form (edp_filtered.cuh): the side of x against each
+// edge is the binary64 sign (0) or the exact one (1, 2; tallied in t by 2).
+template <int F>
+__device__ inline bool contains_flat(const Dev &d, int source, V2 x, Tally &t) {
   const V2 *p = d.src_v + int64_t(kSourceVertices) * source;
   const int n = d.src_n[source];
   for (int j = 0; j < n; ++j) {
     V2 a = p[j], b = p[(j + 1) % n];
-    double s = cross(a, b, x);
+    int stage = 0;
+    const int s = side_sign<F>(a, b, x, stage);
+    if constexpr (F == 2) t.add(stage);
     bool owned = b.y > a.y || (b.y == a.y && b.x < a.x);
-    if (s < 0.0 || (s == 0.0 && !owned)) return false;
+    if (s < 0 || (s == 0 && !owned)) return false;
   }
   return n > 0;
 }
@@ -577,12 +583,14 @@ struct HitBuffer {
 
 // One ray per group leader: up to kCandidatesPerPass sources, the rest of the
 // traversal is queued for the persistent continuation (event_kernels.py:196-245).
+template <int F>
 __global__ void k_ray_hits(Dev d) {
   const int live = live_polygons(d);
   const int leaves = *d.source_tree.size;
   const bool grid = d.sc[kRayGridOn] != 0;
   long long groups = 0, tests = 0, heavy_rays = 0;
   HitBuffer hits;
+  Tally contain;
   for (int64_t k = tid(); k < live; k += stride()) {
     if (d.status[kError] != 0) return;
     const int i = d.order[k];  // spatial order: neighbouring rays read neighbouring data
@@ -603,7 +611,7 @@ __global__ void k_ray_hits(Dev d) {
         if (!overlaps(d.src_lo[s], d.src_hi[s], lo, hi)) continue;
         ++met;
         last = max(last, d.leaf_of[s]);
-        if (contains_flat(d, s, x)) {
+        if (contains_flat<F>(d, s, x, contain)) {
           hits.source[hits.count] = s;
           hits.depth[hits.count] = value(d.scores[s], x);
           ++found;
@@ -623,7 +631,7 @@ __global__ void k_ray_hits(Dev d) {
       node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
       if (s < 0) break;
       ++tests;
-      if (contains_flat(d, s, x)) {
+      if (contains_flat<F>(d, s, x, contain)) {
         hits.source[hits.count] = s;
         hits.depth[hits.count] = value(d.scores[s], x);
         ++hits.count;
@@ -642,6 +650,7 @@ __global__ void k_ray_hits(Dev d) {
   count_add(&d.metrics[kRayGroups], groups);
   count_add(&d.metrics[kRayCandidateTests], tests);
   count_add(&d.metrics[kHeavyRayGroups], heavy_rays);
+  if constexpr (F == 2) contain.flush(d, kPredContain);
 }
 
 // The continuation of the rays whose primary pass did not finish, one warp
@@ -651,6 +660,7 @@ __global__ void k_ray_hits(Dev d) {
 // and the batch's hits go to the shared pool with one reservation.  The
 // candidates, and so the hits, are those of the reference's disjoint-subtree
 // continuation.
+template <int F>
 __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
   const unsigned full = 0xffffffffu;
   if (d.status[kError] != 0) return;
@@ -665,6 +675,7 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
   while (parts * 2LL * jobs <= 32768 && parts * 2 * 32 <= leaves) parts *= 2;
   const int width = leaves / parts;
   long long tests = 0;  // lane 0's tally
+  Tally contain;
   for (int64_t task = tid() >> 5; task < jobs * parts; task += warps) {
     const int2 job = d.heavy_queries[task / parts];
     const int part = int(task % parts), end = (part + 1) * width;
@@ -687,7 +698,7 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
       double depth = 0.0;
       if ((batch >> lane) & 1u) {
         s = __ldg(&d.source_tree.ids[first + lane]);
-        hit = contains_flat(d, s, x);
+        hit = contains_flat<F>(d, s, x, contain);
         if (hit) depth = value(d.scores[s], x);
       }
       const unsigned hits = __ballot_sync(full, hit);
@@ -714,6 +725,7 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
     }
   }
   if (lane == 0) add_metric(d, kRayCandidateTests, tests);
+  if constexpr (F == 2) contain.flush(d, kPredContain);
 }
 
 __global__ void k_check_hits(Dev d) {
@@ -751,33 +763,65 @@ __global__ void k_hit_place(Dev d) {
 // Order each group's hits by (ordered depth bits, source): the order of the
 // three stable radix passes below, whose keys are the same (a source is hit
 // at most once per group, so no two hits of a group tie).
+// The filtered forms (F > 0) order two hits by the exact sign of the
+// difference of their sources' depth planes at the group's sample, equal
+// depths by source: the order the binary64 keys give wherever rounding does
+// not decide it.
+template <int F>
 __global__ void k_group_sort(Dev d) {
   // After a hit-pool overflow the groups' counts exceed the hits stored.
   if (d.sc[kSortHits] != 0 || d.status[kError] != 0) return;
   const int live = live_polygons(d);
+  Tally order;
   for (int64_t g = tid(); g < live; g += stride()) {
     const int k = d.group_counts[g];
     if (k < 2) continue;
     int *ids = d.hit_ids + d.group_offsets[g];
-    unsigned long long key[kGroupSort];
     int src[kGroupSort], id[kGroupSort];
-    for (int j = 0; j < k; ++j) {
-      const int h = ids[j];
-      const unsigned long long kj = ordered_bits(d.hit_depth[h]);
-      const int sj = d.hit_src[h];
-      int m = j - 1;
-      while (m >= 0 && (key[m] > kj || (key[m] == kj && src[m] > sj))) {
-        key[m + 1] = key[m];
-        src[m + 1] = src[m];
-        id[m + 1] = id[m];
-        --m;
+    if constexpr (F == 0) {
+      unsigned long long key[kGroupSort];
+      for (int j = 0; j < k; ++j) {
+        const int h = ids[j];
+        const unsigned long long kj = ordered_bits(d.hit_depth[h]);
+        const int sj = d.hit_src[h];
+        int m = j - 1;
+        while (m >= 0 && (key[m] > kj || (key[m] == kj && src[m] > sj))) {
+          key[m + 1] = key[m];
+          src[m + 1] = src[m];
+          id[m + 1] = id[m];
+          --m;
+        }
+        key[m + 1] = kj;
+        src[m + 1] = sj;
+        id[m + 1] = h;
       }
-      key[m + 1] = kj;
-      src[m + 1] = sj;
-      id[m + 1] = h;
+    } else {
+      const V2 x = d.samples[g];
+      double depth[kGroupSort];
+      for (int j = 0; j < k; ++j) {
+        const int h = ids[j];
+        const double zj = d.hit_depth[h];
+        const int sj = d.hit_src[h];
+        const Plane pj = d.scores[sj];
+        int m = j - 1;
+        while (m >= 0) {
+          int stage = 0;
+          const int o = order_sign<F>(d.scores[src[m]], depth[m], pj, zj, x, stage);
+          if constexpr (F == 2) order.add(stage);
+          if (!(o > 0 || (o == 0 && src[m] > sj))) break;
+          depth[m + 1] = depth[m];
+          src[m + 1] = src[m];
+          id[m + 1] = id[m];
+          --m;
+        }
+        depth[m + 1] = zj;
+        src[m + 1] = sj;
+        id[m + 1] = h;
+      }
     }
     for (int j = 0; j < k; ++j) ids[j] = id[j];
   }
+  if constexpr (F == 2) order.flush(d, kPredOrder);
 }
 
 // Keys of the three stable passes that order hits by (group, depth, source)
@@ -801,13 +845,20 @@ __global__ void k_hit_keys(Dev d, int stage) {
 // Rank = number of the group's hits nearer than the representative's source
 // at this polygon's sample, equal depths ordered by source index
 // (event_kernels.py:342-385).
+// The filtered forms search with the exact order of k_group_sort when the
+// groups were sorted there, and with the binary64 order after the radix
+// passes (groups deeper than kGroupSort), matching the order searched.
+template <int F>
 __global__ void k_assign(Dev d) {
   const int live = live_polygons(d);
+  const bool exact = F != 0 && d.sc[kSortHits] == 0;
+  Tally order;
   for (int64_t i = tid(); i < live; i += stride()) {
     if (d.status[kError] != 0) return;
     int source = d.out_src[d.reps[i]];
     V2 x = d.samples[i];
-    double z = value(d.scores[source], x);
+    const Plane ps = d.scores[source];
+    double z = value(ps, x);
     int g = d.groups[i];
     int low = 0, high = d.group_counts[g];
     const int *ids = d.hit_ids + d.group_offsets[g];
@@ -815,8 +866,18 @@ __global__ void k_assign(Dev d) {
       int mid = (low + high) / 2;
       int h = ids[mid];
       int hs = d.hit_src[h];
-      double hz = value(d.scores[hs], x);
-      if (hz < z || (hz == z && hs < source))
+      const Plane ph = d.scores[hs];
+      double hz = value(ph, x);
+      bool nearer;
+      if (exact) {
+        int stage = 0;
+        const int o = order_sign<F>(ph, hz, ps, z, x, stage);
+        if constexpr (F == 2) order.add(stage);
+        nearer = o < 0 || (o == 0 && hs < source);
+      } else {
+        nearer = hz < z || (hz == z && hs < source);
+      }
+      if (nearer)
         low = mid + 1;
       else
         high = mid;
@@ -831,6 +892,7 @@ __global__ void k_assign(Dev d) {
       atomicMax(&d.status[kLayers], low + 1);
     }
   }
+  if constexpr (F == 2) order.flush(d, kPredOrder);
 }
 
 __global__ void k_layers_reset(Dev d) { d.status[kLayers] = 0; }
@@ -1019,10 +1081,10 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     note_launch();
   }
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_GRID, st));
-  k_ray_hits<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_LAUNCH_FORM(d.predicates, k_ray_hits, blocks(R), kBlock, st, d);
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_PRIMARY, st));
-  k_heavy_hits<<<148 * 16, kBlock, 0, st>>>(d);
+  EDP_LAUNCH_FORM(d.predicates, k_heavy_hits, 148 * 16, kBlock, st, d);
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_HEAVY, st));
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
@@ -1042,12 +1104,12 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   EDP_CHECK(cudaMemsetAsync(d.group_fill, 0, sizeof(int) * R, st));
   k_hit_place<<<blocks(d.cap.hits), kBlock, 0, st>>>(d);
   note_launch();
-  k_group_sort<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_LAUNCH_FORM(d.predicates, k_group_sort, blocks(R), kBlock, st, d);
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_HIT_SORT, st));
   k_layers_reset<<<1, 1, 0, st>>>(d);
   note_launch();
-  k_assign<<<blocks(R), kBlock, 0, st>>>(d);
+  EDP_LAUNCH_FORM(d.predicates, k_assign, blocks(R), kBlock, st, d);
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_ASSIGN, st));
   if (d.merge_regions) {

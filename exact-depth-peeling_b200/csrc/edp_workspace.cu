@@ -86,6 +86,7 @@ cudaError_t allocate_shared(edp_peeler *p) {
                 S = int64_t(kSourceVertices) * n;
   EDP_CHECK(alloc(p, &d.status, kStatusSlots));
   EDP_CHECK(alloc(p, &d.metrics, kMetrics));
+  EDP_CHECK(alloc(p, &d.pred_counts, kPredCounters));
   EDP_CHECK(alloc(p, &d.sc, kScalarCount));
   EDP_CHECK(alloc(p, &d.parity, 1));
   EDP_CHECK(alloc(p, &d.condition, 1));
@@ -446,6 +447,7 @@ int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, i
   d.share_regions = o.share_regions != 0;
   d.propagate_ranks = o.propagate_ranks != 0;
   d.merge_regions = o.merge_regions != 0;
+  d.predicates = EDP_PREDICATES_FILTERED;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = allocate_event(p);
@@ -494,6 +496,7 @@ int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, 
   d.all_layers = layers == 0;
   d.workers = int(c.workers);
   d.pieces = int(c.pieces_per_worker);
+  d.predicates = EDP_PREDICATES_FILTERED;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = allocate_device(p);
@@ -647,6 +650,22 @@ int edp_run_stage(edp_peeler *p, int32_t stage) {
     EDP_TRY(e);
   }
   EDP_TRY(cudaGraphLaunch(p->stage_exec[stage], p->stream));
+  return EDP_OK;
+}
+
+int edp_set_predicates(edp_peeler *p, int32_t mode) {
+  if (!p || mode < EDP_PREDICATES_BINARY64 || mode > EDP_PREDICATES_COUNTED)
+    return EDP_ERR_ARGUMENT;
+  if (p->exec) return EDP_ERR_STATE;  // the captured graph holds the mode it was made with
+  p->d.predicates = mode;
+  return EDP_OK;
+}
+
+int edp_predicate_counts(edp_peeler *p, int64_t *counts) {
+  if (!p || !counts) return EDP_ERR_ARGUMENT;
+  EDP_TRY(cudaStreamSynchronize(p->stream));
+  EDP_TRY(cudaMemcpy(counts, p->d.pred_counts, sizeof(int64_t) * kPredCounters,
+                     cudaMemcpyDeviceToHost));
   return EDP_OK;
 }
 

@@ -8,7 +8,7 @@ import ctypes
 from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libedp_b200.so"
-ABI_VERSION = 3  # EDP_ABI_VERSION in include/edp.h
+ABI_VERSION = 4  # EDP_ABI_VERSION in include/edp.h
 
 I64 = ctypes.c_int64
 I32 = ctypes.c_int32
@@ -45,8 +45,14 @@ EXPORTS = (
     "edp_device_default_capacities", "edp_warmup", "edp_enqueue", "edp_capture", "edp_run",
     "edp_read_status", "edp_get_outputs", "edp_destroy", "edp_status_string",
     "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
-    "edp_last_error_site", "edp_weld_noalloc", "edp_stage_times",
+    "edp_last_error_site", "edp_weld_noalloc", "edp_stage_times", "edp_set_predicates",
+    "edp_predicate_counts",
 )
+
+# enum edp_predicates and enum edp_predicate_class in include/edp.h.
+PREDICATE_MODES = {"binary64": 0, "filtered": 1, "counted": 2}
+PREDICATE_CLASSES = ("side", "segment", "depth", "contain", "order", "clip")
+PREDICATE_STAGES = ("binary32", "binary64", "exact")
 
 # enum edp_stage in include/edp.h, in order (edp_stage_times fills one float each).
 STAGE_NAMES = (
@@ -89,6 +95,8 @@ def load():
     lib.edp_run_stage.argtypes = [P, I32]
     lib.edp_graph_kernels.argtypes = [P, P, P]
     lib.edp_stage_times.argtypes = [P, P]
+    lib.edp_set_predicates.argtypes = [P, I32]
+    lib.edp_predicate_counts.argtypes = [P, P]
     lib.edp_weld_noalloc.argtypes = [P, I64, P, P]
     lib.edp_weld_noalloc.restype = ctypes.c_int
     lib.edp_destroy.argtypes = [P]

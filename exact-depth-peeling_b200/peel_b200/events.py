@@ -53,10 +53,17 @@ class EventPeeler(_Peeler):
     All on one CUDA device.  The caller owns the inputs and may change their
     values (not addresses or sizes) between replays on ``peeler.stream``.
     Inputs must have resolved surface intersections.
+
+    ``predicates`` (not in the reference, whose kernels are plain binary64)
+    selects the sign predicates: "filtered" (exact signs through binary32 and
+    binary64 filters and expansion arithmetic), "binary64" (the reference's
+    plain expressions) or "counted" (filtered, with per-class tallies of the
+    deciding stage, read by ``predicate_counts()``).
     """
 
     def __init__(self, vertices, faces, camera, settings, *, capacities=None, layers=0,
-                 share_regions=True, propagate_ranks=True, merge_regions=False):
+                 share_regions=True, propagate_ranks=True, merge_regions=False,
+                 predicates="filtered"):
         import torch
 
         self.device = _check_inputs(vertices, faces, camera, settings)
@@ -94,6 +101,7 @@ class EventPeeler(_Peeler):
                 "EventPeeler")
         self._ws = _Workspace(handle, self.device, (vertices, faces, camera, settings))
         self._ws.expose(self)
+        self._set_predicates(predicates)
         self.graph = None
         self.warmed = False
 

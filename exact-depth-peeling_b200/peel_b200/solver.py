@@ -172,6 +172,12 @@ class _Workspace:
         with torch.cuda.device(self.device):
             _lib.check(getattr(_lib.load(), name)(self.handle), what)
 
+    def call_args(self, name, what, *args):
+        import torch
+
+        with torch.cuda.device(self.device):
+            _lib.check(getattr(_lib.load(), name)(self.handle, *args), what)
+
     def read(self):
         status = np.zeros(16, dtype=np.int32)
         metrics = np.zeros(METRIC_COUNT, dtype=np.int64)
@@ -222,6 +228,22 @@ class _Peeler:
             self.capture()
         self._ws.call("edp_run", "run")
 
+    def _set_predicates(self, predicates):
+        if predicates not in _lib.PREDICATE_MODES:
+            raise ValueError(f"predicates must be one of {sorted(_lib.PREDICATE_MODES)}")
+        self._ws.call_args("edp_set_predicates", "predicates", _lib.PREDICATE_MODES[predicates])
+        self.predicates = predicates
+
+    def predicate_counts(self):
+        """{class: {stage: calls}} of the last extraction when the peeler was
+        made with predicates="counted" (zeros otherwise); waits for it."""
+        counts = np.zeros(3 * len(_lib.PREDICATE_CLASSES), dtype=np.int64)
+        _lib.check(_lib.load().edp_predicate_counts(self._ws.handle, counts.ctypes.data),
+                   "predicate counts")
+        rows = counts.reshape(-1, 3)
+        return {c: dict(zip(_lib.PREDICATE_STAGES, map(int, row)))
+                for c, row in zip(_lib.PREDICATE_CLASSES, rows)}
+
     def stage_times(self):
         """{stage: device ms} of the last replay of this peeler's own graph
         (run() / capture()), from timing events the graph records at each
@@ -238,7 +260,8 @@ class DevicePeeler(_Peeler):
     that still has unresolved surface crossings.
     """
 
-    def __init__(self, vertices, faces, camera, settings, *, capacities=None, layers=0):
+    def __init__(self, vertices, faces, camera, settings, *, capacities=None, layers=0,
+                 predicates="filtered"):
         import torch
 
         self.device = _check_inputs(vertices, faces, camera, settings)
@@ -267,6 +290,7 @@ class DevicePeeler(_Peeler):
                 "DevicePeeler")
         self._ws = _Workspace(handle, self.device, (vertices, faces, camera, settings))
         self._ws.expose(self)
+        self._set_predicates(predicates)
         self.graph = None
         self.warmed = False
 

@@ -46,7 +46,7 @@ enum edp_status {
 enum {
   EDP_STATUS_SLOTS = 16,
   EDP_METRICS = 20,
-  EDP_ABI_VERSION = 3,
+  EDP_ABI_VERSION = 4,
   EDP_ERR_BIT_POLYGON = 1,
   EDP_ERR_BIT_WORKER = 2,
   EDP_ERR_BIT_RESIDUAL = 4,
@@ -136,6 +136,36 @@ void edp_destroy(edp_peeler *p);
  * captured stage graphs (scripts/profile_events.py:35-98).  Replaying stage 0
  * resets the counters, so run the full graph again before reading outputs. */
 int edp_run_stage(edp_peeler *p, int32_t stage);
+/* Sign predicates of the kernels (orientation, containment, depth order):
+ * the reference's plain binary64 expressions, or exact signs through
+ * escalating filters (binary32 with a static error bound, then binary64, then
+ * exact expansion arithmetic), optionally tallied per class and deciding
+ * stage.  Workspaces start FILTERED.  Constructions stay binary64. */
+enum edp_predicates {
+  EDP_PREDICATES_BINARY64 = 0,
+  EDP_PREDICATES_FILTERED = 1,
+  EDP_PREDICATES_COUNTED = 2
+};
+/* Predicate classes of edp_predicate_counts (three stages each: binary32,
+ * binary64, exact). */
+enum edp_predicate_class {
+  EDP_PRED_SIDE = 0,    /* patch vertex against a contour segment's line */
+  EDP_PRED_SEGMENT,     /* contour segment end against a patch edge */
+  EDP_PRED_DEPTH,       /* patch depth against a segment end's depth */
+  EDP_PRED_CONTAIN,     /* ray sample against a source edge */
+  EDP_PRED_ORDER,       /* depth order of two sources at a ray sample */
+  EDP_PRED_CLIP,        /* clipping piece against an occluder (DevicePeeler) */
+  EDP_PRED_CLASSES
+};
+/* Selects the predicate form (enum edp_predicates) for the next capture or
+ * warm-up; EDP_ERR_STATE once the workspace's own graph exists.  No
+ * counterpart in the reference, whose kernels are plain binary64. */
+int edp_set_predicates(edp_peeler *p, int32_t mode);
+/* counts[3 * class + stage] of the last extraction run with
+ * EDP_PREDICATES_COUNTED (zero otherwise); synchronises the workspace
+ * stream. */
+int edp_predicate_counts(edp_peeler *p, int64_t *counts);
+
 /* Stages timed by edp_stage_times, in extraction order: the reference
  * profiler's phases (scripts/profile_events.py:35-56) with its rank and mesh
  * phases split where this build's kernels split.  The DevicePeeler fills
@@ -199,8 +229,9 @@ const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
 /* Source location ("file:line") of the CUDA call behind the last EDP_ERR_CUDA. */
 const char *edp_last_error_site(void);
-/* EDP_ABI_VERSION of the library: 3 since edp_stage_times; 2 had metrics[]
- * of 20 counters (heavy_noded_polygons added); 1 had 19. */
+/* EDP_ABI_VERSION of the library: 4 since the predicate forms, 3 since
+ * edp_stage_times; 2 had metrics[] of 20 counters (heavy_noded_polygons
+ * added); 1 had 19. */
 int edp_abi_version(void);
 
 #ifdef __cplusplus
