@@ -40,6 +40,7 @@ struct edp_peeler {
   // the end of each EDP_STAGE_*); created with the graph.
   cudaEvent_t marks[EDP_STAGE_COUNT + 1] = {};
   bool marked = false;
+  int64_t bytes = 0;  // device bytes of the pools allocated through alloc()
 };
 
 namespace {
@@ -63,6 +64,7 @@ cudaError_t alloc(edp_peeler *p, T **ptr, int64_t count) {
   cudaError_t e = cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(T) * size_t(count));
   if (e == cudaSuccess) {
     p->allocations.push_back(*ptr);
+    p->bytes += int64_t(sizeof(T)) * count;
     e = cudaMemset(*ptr, 0, sizeof(T) * size_t(count));
   }
   return e;
@@ -666,6 +668,17 @@ int edp_predicate_counts(edp_peeler *p, int64_t *counts) {
   EDP_TRY(cudaStreamSynchronize(p->stream));
   EDP_TRY(cudaMemcpy(counts, p->d.pred_counts, sizeof(int64_t) * kPredCounters,
                      cudaMemcpyDeviceToHost));
+  return EDP_OK;
+}
+
+int edp_workspace_bytes(edp_peeler *p, int64_t *bytes) {
+  if (!p || !bytes) return EDP_ERR_ARGUMENT;
+  int64_t total = p->bytes;
+  for (const TreeBuffers *t : {&p->source_tree, &p->seg_tree, &p->point_tree, &p->residual_tree})
+    if (t->nodes)  // nodes, ids (x2), keys (x2), flags and size
+      total += int64_t(sizeof(float4) * 4 + 2 * sizeof(int) + 2 * sizeof(uint64_t)) *
+                   t->leaves_cap + 3 * int64_t(sizeof(int));
+  *bytes = total;
   return EDP_OK;
 }
 

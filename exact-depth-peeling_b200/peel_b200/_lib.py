@@ -46,7 +46,8 @@ EXPORTS = (
     "edp_read_status", "edp_get_outputs", "edp_destroy", "edp_status_string",
     "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
     "edp_last_error_site", "edp_weld_noalloc", "edp_stage_times", "edp_set_predicates",
-    "edp_predicate_counts",
+    "edp_predicate_counts", "edp_workspace_bytes", "edp_tile_features", "edp_mlp_infer",
+    "edp_mlp_grad", "edp_adam_step",
 )
 
 # enum edp_predicates and enum edp_predicate_class in include/edp.h.
@@ -97,6 +98,11 @@ def load():
     lib.edp_stage_times.argtypes = [P, P]
     lib.edp_set_predicates.argtypes = [P, I32]
     lib.edp_predicate_counts.argtypes = [P, P]
+    lib.edp_workspace_bytes.argtypes = [P, P]
+    lib.edp_tile_features.argtypes = [P, I64, P, I64, P, P, P, P, P]
+    lib.edp_mlp_infer.argtypes = [P, P, I64, P, P]
+    lib.edp_mlp_grad.argtypes = [P, P, P, P, I64, ctypes.c_float, P, P, P]
+    lib.edp_adam_step.argtypes = [P, P, P, P, I64] + [ctypes.c_float] * 4 + [I32, P]
     lib.edp_weld_noalloc.argtypes = [P, I64, P, P]
     lib.edp_weld_noalloc.restype = ctypes.c_int
     lib.edp_destroy.argtypes = [P]

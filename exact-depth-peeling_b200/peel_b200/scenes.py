@@ -210,13 +210,14 @@ def torus(major_segments, minor_segments, major, minor, noise, rng):
     return vertices, faces
 
 
-def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7):
+def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7, direction=None):
     """``count`` noisy spheres and tori (bounding radii log-uniform in
     [0.05, 0.5], faces in proportion to surface area, about ``total_faces`` in
     all), placed without overlap by rejection sampling in a cube that grows
     until they fit, then viewed by a 60 degree pinhole camera at 3x the scene's
-    bounding radius.  Disjoint placement stands in for resolving overlapping
-    primitives, which needs an exact mesh-intersection resolver."""
+    bounding radius from `direction` (default (0.3, 0.4, 3)).  Disjoint
+    placement stands in for resolving overlapping primitives, which needs an
+    exact mesh-intersection resolver."""
     rng = np.random.default_rng(seed)
     radii = np.exp(rng.uniform(np.log(0.05), np.log(0.5), size=count))
     kinds = rng.integers(0, 2, size=count)  # 0 sphere, 1 torus
@@ -251,9 +252,21 @@ def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7):
     faces = np.concatenate(parts_f).astype(np.int32)
     centroid = vertices.mean(0)
     bound = np.linalg.norm(vertices - centroid, axis=1).max()
-    camera, settings = _pinhole(centroid + np.array([0.3, 0.4, 3.0]) / np.linalg.norm([0.3, 0.4, 3.0])
-                                * 3 * bound, centroid, near=0.01 * bound)
+    view = np.array([0.3, 0.4, 3.0]) if direction is None else np.asarray(direction, float)
+    camera, settings = _pinhole(centroid + view / np.linalg.norm(view) * 3 * bound, centroid,
+                                near=0.01 * bound)
     return vertices, faces, camera, settings
+
+
+def training_mesh(seed):
+    """One seeded mesh of the pool-sizing training set: packed primitives
+    (4 to 40 of them, 4,096 to 65,536 faces, log-uniform) seen from a random
+    direction by the 60 degree pinhole camera at 3x the bounding radius."""
+    rng = np.random.default_rng(seed)
+    faces = int(np.exp(rng.uniform(np.log(4096), np.log(65536))))
+    count = int(rng.integers(4, 41))
+    direction = rng.normal(size=3)
+    return packed_primitives(total_faces=faces, count=count, seed=seed, direction=direction)
 
 
 def marching_tetrahedra(field, lo, hi, cells):

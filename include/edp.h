@@ -224,6 +224,39 @@ int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
 #define EDP_WELD_NOALLOC_MAX_VERTICES 262144
 int edp_weld_noalloc(const double *vertices, int64_t nv, int32_t *canonical, void *stream);
 
+/* Device bytes the workspace holds (pools, hierarchies, scratch).  No
+ * counterpart in the reference. */
+int edp_workspace_bytes(edp_peeler *p, int64_t *bytes);
+
+/* Learned pool sizing.  No counterpart in the reference, which sizes every
+ * pool at worst case from the face count (warp_peel/events.py:19-33).
+ *
+ * edp_tile_features projects the mesh into EDP_TILE_AXIS^2 screen tiles and
+ * writes EDP_MLP_INPUTS features per tile (row-major [tiles][inputs]) to
+ * `features`; `scratch` holds EDP_TILE_SCRATCH floats of the caller's device
+ * memory.  edp_mlp_infer evaluates the 16 -> 64 -> 64 -> 3 perceptron on
+ * `rows` feature rows (BF16 weights on the tensor cores, FP32 accumulation);
+ * `params` holds EDP_MLP_PARAMS floats: W1[64][16], b1[64], W2[64][64],
+ * b2[64], W3[3][64], b3[3].  edp_mlp_grad adds the gradient of
+ * sum(mask * (y - target)^2) * scale to `grad` and the unscaled sum to
+ * loss[0]; edp_adam_step applies one Adam step to `params` (moments m, v)
+ * and clears `grad`.  All pointers are device memory; kernels run on
+ * `stream`. */
+#define EDP_TILE_AXIS 16
+#define EDP_MLP_INPUTS 16
+#define EDP_MLP_HIDDEN 64
+#define EDP_MLP_OUTPUTS 3
+#define EDP_MLP_PARAMS 5443
+#define EDP_TILE_SCRATCH (EDP_TILE_AXIS * EDP_TILE_AXIS * 12 + 4)
+int edp_tile_features(const double *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                      const double *camera, const double *settings, float *scratch,
+                      float *features, void *stream);
+int edp_mlp_infer(const float *params, const float *x, int64_t rows, float *y, void *stream);
+int edp_mlp_grad(const float *params, const float *x, const float *target, const float *mask,
+                 int64_t rows, float scale, float *grad, float *loss, void *stream);
+int edp_adam_step(float *params, float *grad, float *m, float *v, int64_t count, float lr,
+                  float beta1, float beta2, float eps, int32_t step, void *stream);
+
 /* Human-readable edp_status; the last CUDA error code of this thread. */
 const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
