@@ -1,5 +1,6 @@
 // Host-side declarations shared by the translation units of libedp_b200.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -115,7 +116,15 @@ enum Scalar : int {
   kSegBig = 19,        // contour segments too large for the grid's cells
   kHeavyPolygons = 20, // polygons queued for warp-wide noding
   kFrontierNext = 8,   // next frontier patch a subdivision warp takes
-  kScalarCount = 24
+  // Iterative clipping (DevicePeeler): live pieces of this round, pieces
+  // appended for the next round, hidden pieces of this layer, the current
+  // work pool, and the clipping-round loop's condition.
+  kClipLive = 21,
+  kClipNext = 22,
+  kClipHidden = 23,
+  kClipParity = 24,
+  kClipCondition = 25,
+  kScalarCount = 28
 };
 
 // Predicate tallies: six classes by three deciding stages (edp_filtered.cuh).
@@ -242,10 +251,21 @@ struct Dev {
   int *res_n[2], *res_src[2];
   float4 *res_lo, *res_hi;
   Tree residual_tree;
-  V2 *pool_v[3];                    // per-worker pieces: visible, temporary, hidden
-  int *pool_n[3];                   // [workers][pieces]
+  // Clipping work: ping-pong pools of live pieces [work_cap][32], each with
+  // its target (a residual patch index) and the position of its candidate
+  // walk; the layer's hidden pieces [hidden_cap][32] with their targets; per
+  // target its visible and hidden piece counts.
+  V2 *work_v[2];
+  int *work_n[2], *work_target[2], *work_cursor[2];
+  int work_cap;
+  V2 *hid_v;
+  int *hid_n, *hid_target;
+  int hidden_cap;
+  int *target_visible, *target_hidden;
   long long *stats;                 // [layers][3]: targets, candidate tests, restored whole
-  int workers, pieces;
+  int workers, pieces;              // clipping threads; pieces one target may hold
+  unsigned long long inner_handle;  // cudaGraphConditionalHandle of the clipping rounds
+  int use_inner;
 };
 
 // Polygon edge `edge` of source `source` is a contour: every edge of a
@@ -265,8 +285,10 @@ cudaError_t stage_prepare_common(const Dev &d, SortScratch &s, TreeBuffers &sour
 cudaError_t stage_device_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
                                  TreeBuffers &contour_tree, cudaStream_t st);
 cudaError_t stage_device_finish(const Dev &d, cudaStream_t st);
+// One layer pass on `st`; its clipping rounds are recorded on `rounds` when
+// `st` is capturing (a nested conditional WHILE node), else host-driven.
 cudaError_t stage_device_layer(const Dev &d, SortScratch &s, TreeBuffers &source_tree,
-                               TreeBuffers &residual_tree, cudaStream_t st);
+                               TreeBuffers &residual_tree, cudaStream_t st, cudaStream_t rounds);
 // Bring the source hierarchy's leaves up to date with its item boxes without
 // re-sorting (solver.py:72-89).
 cudaError_t tree_refit(TreeBuffers &t, const float4 *lo, const float4 *hi, cudaStream_t st);

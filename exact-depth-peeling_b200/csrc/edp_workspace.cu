@@ -24,6 +24,7 @@ struct edp_peeler {
   Dev d{};
   cudaStream_t stream = nullptr;
   cudaStream_t body_stream = nullptr;
+  cudaStream_t round_stream = nullptr;  // records the DevicePeeler's clipping rounds
   SortScratch scratch;
   TreeBuffers source_tree, seg_tree, point_tree;  // seg_tree holds contours for DevicePeeler
   TreeBuffers residual_tree;
@@ -258,8 +259,11 @@ cudaError_t allocate_event(edp_peeler *p) {
 
 cudaError_t allocate_device(edp_peeler *p) {
   Dev &d = p->d;
-  const int64_t n = d.n, F = d.cap.frontier, R = d.cap.regions, E = d.cap.vertices,
-                pool = int64_t(d.workers) * d.pieces;
+  const int64_t n = d.n, F = d.cap.frontier, R = d.cap.regions, E = d.cap.vertices;
+  // Live clipping pieces end as visible (at most R) or hidden (at most F)
+  // pieces, so R + F slots hold every round's queue.
+  d.work_cap = int(std::min<int64_t>(R + F, (int64_t(1) << 31) - 1));
+  d.hidden_cap = int(F);
   EDP_CHECK(allocate_shared(p));
   EDP_CHECK(alloc(p, &d.contour_lo, n));
   EDP_CHECK(alloc(p, &d.contour_hi, n));
@@ -271,10 +275,17 @@ cudaError_t allocate_device(edp_peeler *p) {
   }
   EDP_CHECK(alloc(p, &d.res_lo, F));
   EDP_CHECK(alloc(p, &d.res_hi, F));
-  for (int k = 0; k < 3; ++k) {
-    EDP_CHECK(alloc(p, &d.pool_v[k], pool * kMaxVertices));
-    EDP_CHECK(alloc(p, &d.pool_n[k], pool));
+  for (int k = 0; k < 2; ++k) {
+    EDP_CHECK(alloc(p, &d.work_v[k], int64_t(d.work_cap) * kMaxVertices));
+    EDP_CHECK(alloc(p, &d.work_n[k], d.work_cap));
+    EDP_CHECK(alloc(p, &d.work_target[k], d.work_cap));
+    EDP_CHECK(alloc(p, &d.work_cursor[k], d.work_cap));
   }
+  EDP_CHECK(alloc(p, &d.hid_v, F * kMaxVertices));
+  EDP_CHECK(alloc(p, &d.hid_n, F));
+  EDP_CHECK(alloc(p, &d.hid_target, F));
+  EDP_CHECK(alloc(p, &d.target_visible, F));
+  EDP_CHECK(alloc(p, &d.target_hidden, F));
   EDP_CHECK(alloc(p, &d.stats, 3 * d.cap.layers));
   EDP_CHECK(tree_alloc(p->seg_tree, n));  // the contour hierarchy
   EDP_CHECK(tree_alloc(p->residual_tree, F));
@@ -297,7 +308,8 @@ cudaError_t run_prepare(edp_peeler *p, const Dev &d, cudaStream_t st) {
 }
 cudaError_t run_body(edp_peeler *p, const Dev &d, cudaStream_t st) {
   return p->method == 0 ? stage_step(d, st)
-                        : stage_device_layer(d, p->scratch, p->source_tree, p->residual_tree, st);
+                        : stage_device_layer(d, p->scratch, p->source_tree, p->residual_tree, st,
+                                             p->round_stream);
 }
 cudaError_t run_finish(edp_peeler *p, const Dev &d, cudaStream_t st) {
   if (p->method == 0) {
@@ -501,6 +513,7 @@ int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, 
   d.predicates = EDP_PREDICATES_FILTERED;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->round_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = allocate_device(p);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
@@ -609,6 +622,7 @@ void edp_destroy(edp_peeler *p) {
   tree_free(p->residual_tree);
   for (void *a : p->allocations) cudaFree(a);
   if (p->body_stream) cudaStreamDestroy(p->body_stream);
+  if (p->round_stream) cudaStreamDestroy(p->round_stream);
   for (auto &e : p->stage_exec)
     if (e) cudaGraphExecDestroy(e);
   for (cudaEvent_t ev : p->marks)

@@ -29,6 +29,13 @@ _ERROR_LABELS = {
 
 @dataclass(frozen=True)
 class Capacities:
+    """DevicePeeler pools (warp_peel/solver.py:10-31).  residual: patches
+    left for the next layer; polygons, vertices, triangles: outputs.  The
+    clipping queue shares polygons + residual piece slots among all targets;
+    pieces_per_worker bounds the visible and the hidden pieces of one target
+    (the reference's per-worker pool error); workers is kept for the
+    interface."""
+
     residual: int
     polygons: int
     vertices: int

@@ -71,7 +71,12 @@ typedef struct edp_event_options {
   int32_t share_regions, propagate_ranks, merge_regions;
 } edp_event_options;
 
-/* warp_peel/solver.py:10-31 (Capacities). */
+/* warp_peel/solver.py:10-31 (Capacities).  The same fields, with the
+ * clipping redesigned: the work queue holds polygons + residual pieces and
+ * the hidden pool residual pieces, shared by all targets; pieces_per_worker
+ * bounds the visible and the hidden pieces of one target (error bit 2 above
+ * it, as the reference's per-worker pool); workers is kept for the interface
+ * (the clipping grid is sized for the GPU). */
 typedef struct edp_device_capacities {
   int64_t residual, polygons, vertices, triangles, workers, pieces_per_worker, layers,
       edge_vertices;
