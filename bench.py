@@ -252,7 +252,15 @@ def run_batched(args, rank, world, local_rank):
     torch.cuda.set_device(device)
     host = scenes.CONFIGS[args.config]()
     arrays = [scenes.to_device(h, device) for h in host]
-    batch = BatchPeeler(arrays, fit=True)
+    # Knobs tuned on the batch's first scene, applied to every workspace.
+    from peel_b200 import EventPeeler
+    from peel_b200.autotune import tune
+    from peel_b200.sizing import fit_event_capacities
+
+    _, first_cap = fit_event_capacities(arrays[0])
+    knobs, default_ms, tuned_ms, trials = tune(
+        lambda: EventPeeler(*arrays[0], capacities=first_cap), replays=5)
+    batch = BatchPeeler(arrays, fit=True, tuning=knobs)
     batch.capture()
     meshes = len(batch)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
@@ -347,6 +355,8 @@ def run_batched(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step":
                     int(sum(64 + 152 + 128 * i["triangles"] for i in infos))},
         "gpu_launches": int(args.steps * launches), "clocks": clocks.summary(),
+        "tuning": {"knobs": knobs, "tuned_on": "the batch's first scene",
+                   "default_ms": default_ms, "tuned_ms": tuned_ms, "trials": len(trials)},
         "output": {"polygons": polygons, "triangles": triangles,
                    "layers_max": max(i["layers"] for i in infos)},
         "throughput": {"fragments_per_s": polygons / (ms_per_step * 1e-3),
@@ -397,6 +407,14 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
     arrays = scenes.to_device(host, device)
     p, capacities = fit_event_capacities(arrays)
     lib = _lib.load()
+    # The autotuner's coordinate search over the work-distribution knobs
+    # (same outputs under every choice); the timed replays use its choice.
+    from peel_b200 import EventPeeler
+    from peel_b200.autotune import tune
+
+    knobs, default_ms, tuned_ms, trials = tune(
+        lambda: EventPeeler(*arrays, capacities=capacities), replays=5)
+    p.set_tuning(**knobs)
     p.capture()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
     for _ in range(args.warmup):
@@ -493,6 +511,9 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
                                "rounds": check["rounds"]},
         "clocks": clocks.summary(),
         "stages_ms": stage_ms,
+        "tuning": {"knobs": knobs, "default_ms": default_ms, "tuned_ms": tuned_ms,
+                   "trials": len(trials),
+                   "search": "coordinate search, median of 5 L2-flushed replays per trial"},
         "stages_sum_ms": sum(stage_ms.values()),
         "output": {k: check[k] for k in ("polygons", "triangles", "layers", "boundary_vertices")},
         "throughput": {"fragments_per_s": check["polygons"] / (ms_per_mesh * 1e-3),
@@ -513,6 +534,7 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
         # for the filters' escalation rates.
         del p
         plain, _ = fit_event_capacities(arrays, capacities, predicates="binary64")
+        plain.set_tuning(**knobs)
         plain.capture()
         for _ in range(args.warmup):
             plain.run()

@@ -202,7 +202,7 @@ __global__ void k_active_bounds(Dev d) {
 // pieces: a piece is a convex part of a target with the position of its
 // candidate walk (which hierarchy, and the node the stackless walk resumes
 // at).  Each clipping round runs every queued piece against its next
-// kClipBudget candidates.  A candidate that cuts a piece ends the piece's
+// Dev::clip_budget candidates.  A candidate that cuts a piece ends the piece's
 // round: the parts of the piece outside the candidate (or nearer than it)
 // are queued for the next round with the walk position past the candidate,
 // and the part the candidate hides goes to the layer's hidden pool.  A piece
@@ -214,7 +214,6 @@ __global__ void k_active_bounds(Dev d) {
 // all targets and compacted by atomic appends, so their size follows the
 // pieces alive, not a per-thread reservation.
 
-constexpr int kClipBudget = 32;   // candidate tests per piece and round
 constexpr int kCursorTree = 29;   // walk position: hierarchy << 29 | node
 constexpr int kCursorNode = (1 << kCursorTree) - 1;
 
@@ -441,7 +440,7 @@ __global__ void k_clip_round(Dev d) {
     float4 lo, hi;
     polygon_bounds(p, pn, st, lo, hi);
     lo.z = -1.0e30f;
-    int budget = kClipBudget;
+    int budget = d.clip_budget;
     int result = kKept;
     while (budget > 0) {
       const int tree = cursor >> kCursorTree;

@@ -10,10 +10,10 @@ constexpr int kBlock = 128;
 
 constexpr int kWarps = kBlock / 32;
 constexpr unsigned kFull = 0xffffffffu;
-// Group tests one patch may spend per round before it carries over.  The
-// budget decides only how the work is spread over rounds, never which cut a
-// patch takes: every patch meets its candidates in leaf order in any case.
-constexpr int kStepBudget = 48;
+// Dev::step_budget: group tests one patch may spend per round before it
+// carries over.  The budget decides only how the work is spread over rounds,
+// never which cut a patch takes: every patch meets its candidates in leaf
+// order in any case.
 
 // The smallest power of two holding n lanes: a butterfly over it reduces
 // lanes [0, n), the lanes that hold a patch's vertices.
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
     V2 p = lane < n ? fv[int64_t(kMaxVertices) * i + lane] : v2(0.0, 0.0);
     V2 q = shfl(p, next_lane < n ? next_lane : 0);
     const Plane sc = d.scores[source];
-    int budget = kStepBudget;
+    int budget = d.step_budget;
     float4 lo, hi;
     warp_bounds(p, n, sc, lo, hi);
     lo.z = -1.0e30f;
@@ -417,7 +417,7 @@ __global__ void k_advance(Dev d) {
 
 cudaError_t stage_step(const Dev &d, cudaStream_t st) {
   int64_t g = ceil_div(d.cap.frontier, kWarps);
-  if (g > 148 * 8) g = 148 * 8;
+  if (g > 148 * int64_t(d.subdivide_blocks)) g = 148 * int64_t(d.subdivide_blocks);
   EDP_LAUNCH_FORM(d.predicates, k_subdivide, unsigned(g), kBlock, st, d);
   note_launch();
   k_advance<<<1, 1, 0, st>>>(d);

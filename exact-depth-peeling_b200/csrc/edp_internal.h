@@ -142,6 +142,11 @@ struct Dev {
   // and counted into pred_counts ([class][stage], edp_filtered.cuh).
   int predicates;
   unsigned long long *pred_counts;
+  // Tuning knobs (edp_tuning): subdivision walk steps per patch and round,
+  // subdivision blocks per SM, candidate x edge tests above which a polygon
+  // is noded by a warp, clipping candidate tests per piece and round.  None
+  // changes a result, only how the work is spread.
+  int step_budget, subdivide_blocks, heavy_noding_work, clip_budget;
   Caps cap;
 
   int *status;

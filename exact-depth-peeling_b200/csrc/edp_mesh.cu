@@ -177,8 +177,8 @@ __device__ inline void lift(const Dev &d, V2 x, const Plane &s, double *w) {
 constexpr int kPolygonSplits = 256;  // split points buffered per polygon
 // Candidate points x edges above which a polygon is noded by a whole warp
 // (k_mesh_heavy) rather than by one thread, so that a few large polygons in
-// dense cells do not hold 31 idle lanes of a warp.
-constexpr int kHeavyNodingWork = 1024;
+// dense cells do not hold 31 idle lanes of a warp: Dev::heavy_noding_work
+// (1024 unless tuned).
 
 // The centroid fan of polygon p (n vertices, centroid `center`) through its
 // split points sorted by (edge, parameter).  Counts the fan triangles (signed
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_mesh_polygons(Dev d, int edge_cap
         const int64_t row = (int64_t(layer) * g + cy) * g;
         candidates += d.cell_start[row + cx1 + 1] - d.cell_start[row + cx0];
       }
-      if (candidates * n > kHeavyNodingWork) {
+      if (candidates * n > d.heavy_noding_work) {
         d.heavy_polygons[atomicAdd(&d.sc[kHeavyPolygons], 1)] = int(i);
         continue;
       }

@@ -462,6 +462,10 @@ int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, i
   d.propagate_ranks = o.propagate_ranks != 0;
   d.merge_regions = o.merge_regions != 0;
   d.predicates = EDP_PREDICATES_FILTERED;
+  d.step_budget = 48;
+  d.subdivide_blocks = 8;
+  d.heavy_noding_work = 1024;
+  d.clip_budget = 32;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = allocate_event(p);
@@ -511,6 +515,10 @@ int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, 
   d.workers = int(c.workers);
   d.pieces = int(c.pieces_per_worker);
   d.predicates = EDP_PREDICATES_FILTERED;
+  d.step_budget = 48;
+  d.subdivide_blocks = 8;
+  d.heavy_noding_work = 1024;
+  d.clip_budget = 32;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->round_stream, cudaStreamNonBlocking);
@@ -674,6 +682,42 @@ int edp_set_predicates(edp_peeler *p, int32_t mode) {
     return EDP_ERR_ARGUMENT;
   if (p->exec) return EDP_ERR_STATE;  // the captured graph holds the mode it was made with
   p->d.predicates = mode;
+  return EDP_OK;
+}
+
+int edp_set_tuning(edp_peeler *p, const edp_tuning *t) {
+  if (!p || !t || t->step_budget < 0 || t->subdivide_blocks < 0 || t->subdivide_blocks > 64 ||
+      t->heavy_noding_work < 0 || t->clip_budget < 0)
+    return EDP_ERR_ARGUMENT;
+  if (p->exec) {
+    // The captured graphs hold the knobs they were made with: drop them, and
+    // the next run records the extraction again.
+    EDP_TRY(cudaStreamSynchronize(p->stream));
+    EDP_TRY(cudaGraphExecDestroy(p->exec));
+    EDP_TRY(cudaGraphDestroy(p->graph));
+    p->exec = nullptr;
+    p->graph = nullptr;
+    p->marked = false;
+    for (auto &e : p->stage_exec)
+      if (e) {
+        EDP_TRY(cudaGraphExecDestroy(e));
+        e = nullptr;
+      }
+  }
+  Dev &d = p->d;
+  if (t->step_budget) d.step_budget = t->step_budget;
+  if (t->subdivide_blocks) d.subdivide_blocks = t->subdivide_blocks;
+  if (t->heavy_noding_work) d.heavy_noding_work = t->heavy_noding_work;
+  if (t->clip_budget) d.clip_budget = t->clip_budget;
+  return EDP_OK;
+}
+
+int edp_get_tuning(edp_peeler *p, edp_tuning *t) {
+  if (!p || !t) return EDP_ERR_ARGUMENT;
+  t->step_budget = p->d.step_budget;
+  t->subdivide_blocks = p->d.subdivide_blocks;
+  t->heavy_noding_work = p->d.heavy_noding_work;
+  t->clip_budget = p->d.clip_budget;
   return EDP_OK;
 }
 

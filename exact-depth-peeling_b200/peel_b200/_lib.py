@@ -31,6 +31,11 @@ class DeviceCapacitiesC(ctypes.Structure):
         "layers", "edge_vertices")]
 
 
+class TuningC(ctypes.Structure):
+    _fields_ = [(n, I32) for n in (
+        "step_budget", "subdivide_blocks", "heavy_noding_work", "clip_budget")]
+
+
 class OutputsC(ctypes.Structure):
     _fields_ = [
         ("status", P), ("metrics", P), ("output_vertices", P), ("output_sizes", P),
@@ -47,7 +52,7 @@ EXPORTS = (
     "edp_last_cuda_error", "edp_abi_version", "edp_run_stage", "edp_graph_kernels",
     "edp_last_error_site", "edp_weld_noalloc", "edp_stage_times", "edp_set_predicates",
     "edp_predicate_counts", "edp_workspace_bytes", "edp_tile_features", "edp_mlp_infer",
-    "edp_mlp_grad", "edp_adam_step",
+    "edp_mlp_grad", "edp_adam_step", "edp_set_tuning", "edp_get_tuning",
 )
 
 # enum edp_predicates and enum edp_predicate_class in include/edp.h.
@@ -99,6 +104,8 @@ def load():
     lib.edp_set_predicates.argtypes = [P, I32]
     lib.edp_predicate_counts.argtypes = [P, P]
     lib.edp_workspace_bytes.argtypes = [P, P]
+    lib.edp_set_tuning.argtypes = [P, ctypes.POINTER(TuningC)]
+    lib.edp_get_tuning.argtypes = [P, ctypes.POINTER(TuningC)]
     lib.edp_tile_features.argtypes = [P, I64, P, I64, P, P, P, P, P]
     lib.edp_mlp_infer.argtypes = [P, P, I64, P, P]
     lib.edp_mlp_grad.argtypes = [P, P, P, P, I64, ctypes.c_float, P, P, P]

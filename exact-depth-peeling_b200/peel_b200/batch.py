@@ -17,9 +17,10 @@ class BatchPeeler:
     ``capacities``: one ``EventCapacities`` for all, a list with one per
     scene, or None for ``EventCapacities.for_mesh``; ``fit=True`` sizes each
     workspace from a trial extraction (``sizing.fit_event_capacities``)
-    instead.  Other keyword options go to every ``EventPeeler``."""
+    instead.  ``tuning``: work-distribution knobs (``autotune``) for every
+    workspace.  Other keyword options go to every ``EventPeeler``."""
 
-    def __init__(self, scenes, *, capacities=None, fit=False, **options):
+    def __init__(self, scenes, *, capacities=None, fit=False, tuning=None, **options):
         import torch
 
         scenes = list(scenes)
@@ -37,6 +38,10 @@ class BatchPeeler:
             self.peelers = [fit_event_capacities(s, c, **options)[0] for s, c in zip(scenes, caps)]
         else:
             self.peelers = [EventPeeler(*s, capacities=c, **options) for s, c in zip(scenes, caps)]
+        self.tuning = dict(tuning or {})
+        if self.tuning:
+            for p in self.peelers:
+                p.set_tuning(**self.tuning)
         self.device = self.peelers[0].device
         self.stream = torch.cuda.Stream(self.device)
         self.graph = None

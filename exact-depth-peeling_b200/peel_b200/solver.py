@@ -235,6 +235,23 @@ class _Peeler:
             self.capture()
         self._ws.call("edp_run", "run")
 
+    def set_tuning(self, **knobs):
+        """Work-distribution knobs (edp_tuning in edp.h: step_budget,
+        subdivide_blocks, heavy_noding_work, clip_budget); none changes a
+        result.  The peeler's graph is recorded again by the next run()."""
+        unknown = set(knobs) - {f for f, _ in _lib.TuningC._fields_}
+        if unknown:
+            raise ValueError(f"unknown tuning knobs: {sorted(unknown)}")
+        t = _lib.TuningC(*[int(knobs.get(f, 0)) for f, _ in _lib.TuningC._fields_])
+        self._ws.call_args("edp_set_tuning", "tuning", ctypes.byref(t))
+        self.graph = None  # the workspace dropped its graph; run() records it again
+
+    def tuning(self):
+        """The knobs the workspace uses (dict)."""
+        t = _lib.TuningC()
+        _lib.check(_lib.load().edp_get_tuning(self._ws.handle, ctypes.byref(t)), "tuning")
+        return {f: int(getattr(t, f)) for f, _ in _lib.TuningC._fields_}
+
     def _set_predicates(self, predicates):
         if predicates not in _lib.PREDICATE_MODES:
             raise ValueError(f"predicates must be one of {sorted(_lib.PREDICATE_MODES)}")

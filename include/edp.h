@@ -171,6 +171,25 @@ int edp_set_predicates(edp_peeler *p, int32_t mode);
  * stream. */
 int edp_predicate_counts(edp_peeler *p, int64_t *counts);
 
+/* Work-distribution knobs, read at the next capture or warm-up (0 keeps the
+ * current value); setting them drops the workspace's own graph, which the
+ * next edp_run records again.  None changes a result; the autotuner (peel_b200.autotune)
+ * times replays under each and keeps the fastest.  No counterpart in the
+ * reference, whose kernels fix them (frontier.py:149 and kernels.py:815-908
+ * use 32 candidates per round and 4096 persistent workers).
+ *   step_budget        subdivision: hierarchy walk steps a patch spends in a
+ *                      round before it carries over (default 48)
+ *   subdivide_blocks   subdivision: blocks of 4 warps per SM (default 8)
+ *   heavy_noding_work  noding: candidate x edge tests above which a polygon
+ *                      is noded by a warp instead of a thread (default 1024)
+ *   clip_budget        DevicePeeler: candidate tests per piece and clipping
+ *                      round (default 32) */
+typedef struct edp_tuning {
+  int32_t step_budget, subdivide_blocks, heavy_noding_work, clip_budget;
+} edp_tuning;
+int edp_set_tuning(edp_peeler *p, const edp_tuning *t);
+int edp_get_tuning(edp_peeler *p, edp_tuning *t);
+
 /* Stages timed by edp_stage_times, in extraction order: the reference
  * profiler's phases (scripts/profile_events.py:35-56) with its rank and mesh
  * phases split where this build's kernels split.  The DevicePeeler fills
