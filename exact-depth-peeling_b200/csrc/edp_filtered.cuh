@@ -20,7 +20,7 @@ namespace edp {
 enum PredClass : int {
   kPredSide = 0,     // patch vertex against a contour segment's line (subdivision)
   kPredSegment = 1,  // contour segment end against a patch edge (subdivision)
-  kPredDepth = 2,    // patch depth against a segment end's depth (subdivision)
+  kPredDepth = 2,    // patch plane against a segment end's near plane (subdivision)
   kPredContain = 3,  // sample point against a source edge (ray hits)
   kPredOrder = 4,    // depth order of two sources at a sample (hit order, ranks)
   kPredClip = 5,     // piece against occluder edges and depth (iterative clipping)
@@ -71,27 +71,20 @@ __device__ inline int side_sign(V2 a, V2 b, V2 c, int &stage) {
   }
 }
 
-// Sign of s(x) - offset: the depth plane s at x against a depth.
-template <int F>
-__device__ inline int plane_sign(const Plane &s, V2 x, double offset, int &stage) {
-  if constexpr (F == 0) {
-    return sign_of(value(s, x) - offset);
-  } else {
-    const double p[4] = {s.a, s.b, s.c, offset};
-    const double q[4] = {x.x, x.y, 1.0, -1.0};
-    return pred::dot_sign(p, q, 4, &stage);
-  }
-}
-
 // Sign of s1(x) - s2(x): positive when source 1 lies behind source 2 at x.
 // z1, z2 are the binary64 depths value(s1, x), value(s2, x), which the plain
-// form compares.
+// form compares.  Two identical planes are equal without arithmetic (counted
+// as decided in the first stage).
 template <int F>
 __device__ inline int order_sign(const Plane &s1, double z1, const Plane &s2, double z2, V2 x,
                                  int &stage) {
   if constexpr (F == 0) {
     return sign_of(z1 - z2);
   } else {
+    if (s1.a == s2.a && s1.b == s2.b && s1.c == s2.c) {  // one plane: equal everywhere
+      stage = pred::kBinary32;
+      return 0;
+    }
     const double p[6] = {s1.a, s1.b, s1.c, s2.a, s2.b, s2.c};
     const double q[6] = {x.x, x.y, 1.0, -x.x, -x.y, -1.0};
     return pred::dot_sign(p, q, 6, &stage);

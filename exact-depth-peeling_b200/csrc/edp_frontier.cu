@@ -68,6 +68,8 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
 struct Segments {
   const int *ids;
   const V2 *a, *b, *near;
+  const int2 *near_src;  // the sources whose planes give `near`
+  const Plane *scores;
 };
 
 // Predicate tallies of one subdivision warp (counted form only).
@@ -88,11 +90,13 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
   const bool mine = lane < n;
   const int width = lane_width(n);
   V2 ca = v2(0.0, 0.0), cb = ca, cn = ca;
+  int2 cs = make_int2(0, 0);
   if ((batch >> lane) & 1u) {
     const int c = __ldg(&g.ids[first + lane]);
     ca = g.a[c];
     cb = g.b[c];
     cn = g.near[c];
+    if constexpr (F != 0) cs = g.near_src[c];
   }
   while (batch) {
     const int k = __ffs(int(batch)) - 1;
@@ -116,9 +120,13 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
       sza = sign_of(za);
       szb = sign_of(zb);
     } else {
+      // The patch's depth plane against the plane of the source that gives
+      // the segment its near depth, both at the segment's ends: exact, and
+      // zero when that source is the patch's own.
       int stage_b = 0;
-      sza = plane_sign<F>(sc, a, near.x, stage);
-      szb = plane_sign<F>(sc, b, near.y, stage_b);
+      const int sa = __shfl_sync(kFull, cs.x, k), sb = __shfl_sync(kFull, cs.y, k);
+      sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
+      szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
       if constexpr (F == 2) {
         if (lane == 0) {  // the same test on every lane: count it once
           tally.depth.add(stage);
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
   const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
   const int leaves = *d.seg_tree.size;
   const int next_lane = lane + 1;
-  const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near};
+  const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near, d.seg_near_src, d.scores};
   const Frontier next{d.fv[par ^ 1], d.fn[par ^ 1], d.fsrc[par ^ 1], d.fcur[par ^ 1],
                       &d.status[kNextResidual], d.status, d.cap.frontier};
   long long visits = 0, tests = 0, splits = 0;  // lane 0's tallies

@@ -174,9 +174,11 @@ struct Dev {
   V2 *slot_a, *slot_b;      // per candidate slot (8 per source): canonical end points
   int *seg_flag, *seg_pos;  // per slot: representative of its group, its compact index
   double *seg_za, *seg_zb;  // per table slot: minimum endpoint depths
+  int *seg_srca, *seg_srcb; // per table slot: smallest source attaining each minimum
   // Distinct segments, compacted in slot order: end points, (near depth a, near
   // depth b) and boxes; the contour hierarchy is built over these.
   V2 *seg_a, *seg_b, *seg_near;
+  int2 *seg_near_src;  // the sources whose depth planes give seg_near (exact depth tests)
   float4 *seg_lo, *seg_hi;
   int *seg_table, *seg_min, *seg_slot;
   int seg_mask;

@@ -325,10 +325,18 @@ __global__ void k_segments(Dev d) {
 }
 
 // The first slot of each group represents it (event_kernels.py:440-501).
+// Each member whose endpoint depth is the group's minimum offers its source,
+// the smallest of which the exact depth tests evaluate.
 __global__ void k_segment_flags(Dev d) {
   const int64_t total = int64_t(kSourceVertices) * d.n;
   for (int64_t i = tid(); i < total; i += stride()) {
     const int slot = d.seg_slot[i];
+    if (slot >= 0) {
+      const int source = int(i / kSourceVertices);
+      const Plane sc = d.scores[source];
+      if (value(sc, d.slot_a[i]) == d.seg_za[slot]) atomicMin(&d.seg_srca[slot], source);
+      if (value(sc, d.slot_b[i]) == d.seg_zb[slot]) atomicMin(&d.seg_srcb[slot], source);
+    }
     const bool first = slot >= 0 && d.seg_min[slot] == int(i);
     d.seg_flag[i] = first ? 1 : 0;
     count_add(&d.metrics[kUniqueContours], first ? 1 : 0);
@@ -348,6 +356,7 @@ __global__ void k_segment_compact(Dev d) {
     d.seg_a[c] = a;
     d.seg_b[c] = b;
     d.seg_near[c] = v2(za, zb);
+    d.seg_near_src[c] = make_int2(d.seg_srca[slot], d.seg_srcb[slot]);
     d.seg_lo[c] = make_float4(float(fmin(a.x, b.x) - 2.0e-7), float(fmin(a.y, b.y) - 2.0e-7),
                               float(fmin(za, zb) - pz), 0.f);
     d.seg_hi[c] = make_float4(float(fmax(a.x, b.x) + 2.0e-7), float(fmax(a.y, b.y) + 2.0e-7),
@@ -425,6 +434,8 @@ cudaError_t stage_prepare(const Dev &d, SortScratch &s, TreeBuffers &source_tree
   // 0x7f bytes are 1.38e306 as binary64: above every finite depth we store.
   EDP_CHECK(cudaMemsetAsync(d.seg_za, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
   EDP_CHECK(cudaMemsetAsync(d.seg_zb, 0x7f, sizeof(double) * (int64_t(d.seg_mask) + 1), st));
+  EDP_CHECK(cudaMemsetAsync(d.seg_srca, 0x7f, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
+  EDP_CHECK(cudaMemsetAsync(d.seg_srcb, 0x7f, sizeof(int) * (int64_t(d.seg_mask) + 1), st));
   if (d.n > 0) {
     k_segments<<<blocks(kSourceVertices * int64_t(d.n)), kBlock, 0, st>>>(d);
     note_launch();

@@ -184,11 +184,14 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.seg_a, S));
   EDP_CHECK(alloc(p, &d.seg_b, S));
   EDP_CHECK(alloc(p, &d.seg_near, S));
+  EDP_CHECK(alloc(p, &d.seg_near_src, S));
   EDP_CHECK(alloc(p, &d.seg_lo, S));
   EDP_CHECK(alloc(p, &d.seg_hi, S));
   EDP_CHECK(alloc(p, &d.seg_slot, S));
   EDP_CHECK(alloc(p, &d.seg_za, int64_t(d.seg_mask) + 1));
   EDP_CHECK(alloc(p, &d.seg_zb, int64_t(d.seg_mask) + 1));
+  EDP_CHECK(alloc(p, &d.seg_srca, int64_t(d.seg_mask) + 1));
+  EDP_CHECK(alloc(p, &d.seg_srcb, int64_t(d.seg_mask) + 1));
   EDP_CHECK(alloc(p, &d.seg_table, int64_t(d.seg_mask) + 1));
   EDP_CHECK(alloc(p, &d.seg_min, int64_t(d.seg_mask) + 1));
   for (int k = 0; k < 2; ++k) {

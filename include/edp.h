@@ -156,7 +156,7 @@ enum edp_predicates {
 enum edp_predicate_class {
   EDP_PRED_SIDE = 0,    /* patch vertex against a contour segment's line */
   EDP_PRED_SEGMENT,     /* contour segment end against a patch edge */
-  EDP_PRED_DEPTH,       /* patch depth against a segment end's depth */
+  EDP_PRED_DEPTH,       /* patch plane against a segment end's near plane */
   EDP_PRED_CONTAIN,     /* ray sample against a source edge */
   EDP_PRED_ORDER,       /* depth order of two sources at a ray sample */
   EDP_PRED_CLIP,        /* clipping piece against an occluder (DevicePeeler) */

@@ -49,7 +49,7 @@ def test_capture_contract(tmp_path, monkeypatch, method):
     p = peeler_type(method)(*arrays)
     p.warmup()
     p.stream.synchronize()
-    graph = torch.cuda.CUDAGraph()
+    graph = torch.cuda.CUDAGraph(keep_graph=True)  # keep the cudaGraph_t to print it
     graph.enable_debug_mode()
 
     def forbidden(*_a, **_k):
@@ -65,6 +65,7 @@ def test_capture_contract(tmp_path, monkeypatch, method):
                                 (torch.cuda.Event, "synchronize")):
                 m.setattr(owner, name, forbidden)
             p.enqueue()
+    graph.instantiate()
     graph.replay()
     parity.check_against_oracle(p, data, labels)
     dot = tmp_path / "graph.dot"
