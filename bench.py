@@ -33,6 +33,7 @@ UNIT = "ms/mesh"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 REFERENCE_BUDGET_S = 60.0  # CPU seconds of timed extractions in the reference arm
+DEFAULT_FORM = "filtered"  # the predicate form of EventPeeler's default
 
 
 DESCRIPTIONS = {
@@ -552,27 +553,32 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
             "scene_extent", "max_rel_error")}
         result["vertex_error_max"] = report["max_rel_error"]
     if compare_forms:
-        # The same extraction with the reference's plain binary64 predicates
-        # (the comparator of the filtered form), and one counted extraction
-        # for the filters' escalation rates.
+        # The same extraction under the other predicate forms: the
+        # reference's plain binary64 signs (the comparator of the filtered
+        # forms) and the other exact form, then one counted extraction for
+        # the filters' escalation rates.
         del p
-        plain, _ = fit_event_capacities(arrays, capacities, predicates="binary64")
-        plain.set_tuning(**knobs)
-        plain.capture()
-        for _ in range(args.warmup):
-            plain.run()
-        plain_ms = time_replays(plain, steps, flush)
-        plain_info = plain.read_status()
-        del plain
+        timed = {}
+        for form in ("binary64", "filtered", "filtered64"):
+            if form == DEFAULT_FORM:
+                continue
+            other, _ = fit_event_capacities(arrays, capacities, predicates=form)
+            other.set_tuning(**knobs)
+            other.capture()
+            for _ in range(args.warmup):
+                other.run()
+            ms = time_replays(other, steps, flush)
+            info = other.read_status()
+            timed[form] = {"ms": ms, "output": {k: info[k] for k in ("polygons", "triangles",
+                                                                     "layers")}}
+            del other
         counted, _ = fit_event_capacities(arrays, capacities, predicates="counted")
         counted.run()
         counts = counted.predicate_counts()
         del counted
         result["predicates"] = {
-            "form": "filtered",
-            "filtered_ms": ms_per_mesh, "binary64_ms": plain_ms,
-            "binary64_over_filtered": plain_ms / ms_per_mesh,
-            "binary64_output": {k: plain_info[k] for k in ("polygons", "triangles", "layers")},
+            "form": DEFAULT_FORM, "ms": ms_per_mesh, "others": timed,
+            "binary64_over_default": timed["binary64"]["ms"] / ms_per_mesh,
             "counts": counts,
             "escalated_share": {c: (v["binary64"] + v["exact"]) / max(1, sum(v.values()))
                                 for c, v in counts.items()},

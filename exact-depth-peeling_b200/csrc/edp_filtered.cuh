@@ -7,7 +7,9 @@
 //      certifies it, else in binary64 under Shewchuk's bound, else exactly in
 //      expansion arithmetic (edp_predicates.cuh);
 //   2  filtered and counted: as 1, and every call is tallied by predicate
-//      class and deciding stage into Dev::pred_counts.
+//      class and deciding stage into Dev::pred_counts;
+//   3  filtered from binary64: the same exact signs with the binary32 stage
+//      skipped (the binary64 filter first, then expansion arithmetic).
 // Constructions (intersection points, clip parameters, depths stored for the
 // hit sort's radix fallback) stay binary64 in every form.
 #pragma once
@@ -67,7 +69,7 @@ __device__ inline int side_sign(V2 a, V2 b, V2 c, int &stage) {
   if constexpr (F == 0) {
     return sign_of(cross(a, b, c));
   } else {
-    return pred::orient2d(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
+    return pred::orient2d(a.x, a.y, b.x, b.y, c.x, c.y, &stage, F != 3);
   }
 }
 
@@ -87,7 +89,7 @@ __device__ inline int order_sign(const Plane &s1, double z1, const Plane &s2, do
     }
     const double p[6] = {s1.a, s1.b, s1.c, s2.a, s2.b, s2.c};
     const double q[6] = {x.x, x.y, 1.0, -x.x, -x.y, -1.0};
-    return pred::dot_sign(p, q, 6, &stage);
+    return pred::dot_sign(p, q, 6, &stage, F != 3);
   }
 }
 
@@ -107,7 +109,8 @@ __device__ inline double crossing(double u, double v) {
     switch (form) {                                                      \
       case 0: kernel<0><<<grid, block, 0, stream>>>(__VA_ARGS__); break; \
       case 1: kernel<1><<<grid, block, 0, stream>>>(__VA_ARGS__); break; \
-      default: kernel<2><<<grid, block, 0, stream>>>(__VA_ARGS__); break; \
+      case 2: kernel<2><<<grid, block, 0, stream>>>(__VA_ARGS__); break; \
+      default: kernel<3><<<grid, block, 0, stream>>>(__VA_ARGS__); break; \
     }                                                                    \
   } while (0)
 

@@ -73,8 +73,10 @@ EDP_HD inline int expansion_sign(const double *e, int n) {
 
 // Sign of the doubled signed area of (a, b, c): of
 // (bx - ax)(cy - ay) - (by - ay)(cx - ax), positive when c lies left of a->b.
+// With first32 false the binary32 stage is skipped (the binary64 filter
+// decides first); the sign is the same.
 EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx, double cy,
-                           int *stage = nullptr) {
+                           int *stage = nullptr, bool first32 = true) {
   // Binary32 stage: differences in binary64 (relative error <= 2^-53), then
   // converted, multiplied and subtracted in binary32.  For exact products
   // p1, p2 with S = |p1| + |p2|, each rounded product carries a relative
@@ -89,7 +91,7 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
     const double m = fabs(v);
     return m == 0.0 || (m >= lo && m <= hi);
   };
-  if (in_range(dx1) && in_range(dy1) && in_range(dx2) && in_range(dy2)) {
+  if (first32 && in_range(dx1) && in_range(dy1) && in_range(dx2) && in_range(dy2)) {
     const float f1 = float(dx1) * float(dy2);
     const float f2 = float(dy1) * float(dx2);
     const float det32 = f1 - f2;
@@ -150,7 +152,8 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
 
 // Sign of sum_k p[k] q[k] for n <= 8 terms (a plane evaluated at a point, or
 // the difference of two planes there: the depth order of two sources).
-EDP_HD inline int dot_sign(const double *p, const double *q, int n, int *stage = nullptr) {
+EDP_HD inline int dot_sign(const double *p, const double *q, int n, int *stage = nullptr,
+                           bool first32 = true) {
   // Binary32 stage: inputs rounded (relative error <= u each), products
   // (u) and a sequential sum of n terms (the classical bound (n - 1) u on
   // the absolute values): the computed sum is within (n + 2) u S (1 + O(u))
@@ -158,7 +161,7 @@ EDP_HD inline int dot_sign(const double *p, const double *q, int n, int *stage =
   // stage decides when |sum32| exceeds 2 (n + 3) u s32.  Inputs outside
   // [2^-60, 2^60] (zero excepted) skip it.
   const double lo = 8.673617379884035e-19, hi = 1.152921504606847e18;
-  bool ok = true;
+  bool ok = first32;
   for (int k = 0; k < n && ok; ++k) {
     const double a = fabs(p[k]), b = fabs(q[k]);
     ok = (a == 0.0 || (a >= lo && a <= hi)) && (b == 0.0 || (b >= lo && b <= hi));

@@ -681,7 +681,7 @@ int edp_run_stage(edp_peeler *p, int32_t stage) {
 }
 
 int edp_set_predicates(edp_peeler *p, int32_t mode) {
-  if (!p || mode < EDP_PREDICATES_BINARY64 || mode > EDP_PREDICATES_COUNTED)
+  if (!p || mode < EDP_PREDICATES_BINARY64 || mode > EDP_PREDICATES_FILTERED64)
     return EDP_ERR_ARGUMENT;
   if (p->exec) return EDP_ERR_STATE;  // the captured graph holds the mode it was made with
   p->d.predicates = mode;

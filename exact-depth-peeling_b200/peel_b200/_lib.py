@@ -56,7 +56,7 @@ EXPORTS = (
 )
 
 # enum edp_predicates and enum edp_predicate_class in include/edp.h.
-PREDICATE_MODES = {"binary64": 0, "filtered": 1, "counted": 2}
+PREDICATE_MODES = {"binary64": 0, "filtered": 1, "counted": 2, "filtered64": 3}
 PREDICATE_CLASSES = ("side", "segment", "depth", "contain", "order", "clip")
 PREDICATE_STAGES = ("binary32", "binary64", "exact")
 

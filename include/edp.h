@@ -148,8 +148,9 @@ int edp_run_stage(edp_peeler *p, int32_t stage);
  * stage.  Workspaces start FILTERED.  Constructions stay binary64. */
 enum edp_predicates {
   EDP_PREDICATES_BINARY64 = 0,
-  EDP_PREDICATES_FILTERED = 1,
-  EDP_PREDICATES_COUNTED = 2
+  EDP_PREDICATES_FILTERED = 1,   /* binary32 filter, binary64 filter, exact */
+  EDP_PREDICATES_COUNTED = 2,    /* FILTERED, tallied per class and stage */
+  EDP_PREDICATES_FILTERED64 = 3  /* binary64 filter, exact (same signs) */
 };
 /* Predicate classes of edp_predicate_counts (three stages each: binary32,
  * binary64, exact). */

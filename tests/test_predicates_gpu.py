@@ -10,7 +10,7 @@ import parity
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-FORMS = ["filtered", "binary64", "counted"]
+FORMS = ["filtered", "binary64", "counted", "filtered64"]
 
 
 @pytest.fixture(scope="module", autouse=True)
