@@ -24,8 +24,9 @@ __device__ inline V2 shfl(V2 x, int lane) {
 }
 
 // polygon_bounds() of the patch held one vertex per lane (min and max are
-// exact, so the butterfly order does not matter).
-__device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4 &lo, float4 &hi) {
+// exact, so the butterfly order does not matter).  The plane comes and the
+// box goes by value, which keeps this out-of-line helper's call frame small.
+__device__ __noinline__ Box warp_bounds(V2 p, int n, Plane score) {
   const bool mine = int(threadIdx.x & 31) < n;
   const double z = value(score, p);
   double lx = mine ? p.x : 1.0e30, ly = mine ? p.y : 1.0e30, lz = mine ? z : 1.0e30;
@@ -48,8 +49,8 @@ __device__ __noinline__ void warp_bounds(V2 p, int n, const Plane &score, float4
   hy = __shfl_sync(kFull, hy, 0);
   hz = __shfl_sync(kFull, hz, 0);
   double pz = 2.0e-7 * fmax(1.0, fmax(fabs(lz), fabs(hz)));
-  lo = make_float4(float(lx - 2.0e-7), float(ly - 2.0e-7), float(lz - pz), 0.f);
-  hi = make_float4(float(hx + 2.0e-7), float(hy + 2.0e-7), float(hz + pz), 0.f);
+  return Box{make_float4(float(lx - 2.0e-7), float(ly - 2.0e-7), float(lz - pz), 0.f),
+             make_float4(float(hx + 2.0e-7), float(hy + 2.0e-7), float(hz + pz), 0.f)};
 }
 
 // Does segment a->b cut the patch?  Its line has patch vertices strictly on
@@ -308,7 +309,7 @@ __device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int
 // met every candidate is final and goes to the output pool; one that spends
 // its budget carries over.  Warps take patches from a shared counter.
 template <int F>
-__global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
+__global__ void __launch_bounds__(kBlock, F == 0 ? 5 : 4) k_subdivide(Dev d) {
   __shared__ V2 s_parts[kWarps][2][kMaxVertices];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   V2 *left_part = s_parts[warp][0], *right_part = s_parts[warp][1];
@@ -341,7 +342,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
     const Plane sc = d.scores[source];
     int budget = d.step_budget;
     float4 lo, hi;
-    warp_bounds(p, n, sc, lo, hi);
+    {
+      const Box box = warp_bounds(p, n, sc);
+      lo = box.lo;
+      hi = box.hi;
+    }
     lo.z = -1.0e30f;
     WarpWalk w;
     walk_begin(w, d.seg_tree, leaves, lo, hi, cursor);
@@ -387,7 +392,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_subdivide(Dev d) {
         p = pl;
         n = nl;
         q = shfl(p, next_lane < n ? next_lane : 0);
-        warp_bounds(p, n, sc, lo, hi);
+        {
+      const Box box = warp_bounds(p, n, sc);
+      lo = box.lo;
+      hi = box.hi;
+    }
         lo.z = -1.0e30f;
       }
       w.set_pending(walk_test(d.seg_tree, leaves, w, lo, hi, cursor));

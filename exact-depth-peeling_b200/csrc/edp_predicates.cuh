@@ -18,8 +18,10 @@
 
 #ifdef __CUDACC__
 #define EDP_HD __host__ __device__
+#define EDP_COLD __noinline__
 #else
 #define EDP_HD
+#define EDP_COLD __attribute__((noinline))
 #endif
 
 namespace edp {
@@ -70,6 +72,28 @@ EDP_HD inline int expansion_sign(const double *e, int n) {
 }
 
 // ---------------------------------------------------------------- orient2d
+
+// Exact stage of orient2d: the determinant is ax by - ay bx + bx cy - by cx +
+// cx ay - cy ax; each product is exactly a two-component expansion, and
+// growing one expansion by all twelve components keeps the sum exact.  Out
+// of line: it is rare, and its expansion would otherwise take registers
+// from every caller.
+EDP_HD EDP_COLD int orient2d_exact(double ax, double ay, double bx, double by, double cx,
+                                   double cy) {
+  double e[12];
+  int n = 0;
+  const double xs[6] = {ax, -ay, bx, -by, cx, -cy};
+  const double ys[6] = {by, bx, cy, cx, ay, ax};
+  for (int k = 0; k < 6; ++k) {
+    double x, y;
+    two_product(xs[k], ys[k], x, y);
+    grow(e, n, y);
+    ++n;
+    grow(e, n, x);
+    ++n;
+  }
+  return expansion_sign(e, n);
+}
 
 // Sign of the doubled signed area of (a, b, c): of
 // (bx - ax)(cy - ay) - (by - ay)(cx - ax), positive when c lies left of a->b.
@@ -129,26 +153,27 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
     if (stage) *stage = kBinary64;
     return sign_of(det);
   }
-  // Exact stage: the determinant is ax by - ay bx + bx cy - by cx + cx ay -
-  // cy ax; each product is exactly a two-component expansion, and growing
-  // one expansion by all twelve components keeps the sum exact.
-  double e[12];
-  int n = 0;
-  const double xs[6] = {ax, -ay, bx, -by, cx, -cy};
-  const double ys[6] = {by, bx, cy, cx, ay, ax};
-  for (int k = 0; k < 6; ++k) {
-    double x, y;
-    two_product(xs[k], ys[k], x, y);
-    grow(e, n, y);
-    ++n;
-    grow(e, n, x);
-    ++n;
-  }
   if (stage) *stage = kExact;
-  return expansion_sign(e, n);
+  return orient2d_exact(ax, ay, bx, by, cx, cy);
 }
 
 // ---------------------------------------------------------------- linear forms
+
+// Exact stage of dot_sign: every product as a two-component expansion, all
+// grown into one (out of line, as orient2d_exact).
+EDP_HD EDP_COLD int dot_sign_exact(const double *p, const double *q, int n) {
+  double e[16];
+  int m = 0;
+  for (int k = 0; k < n; ++k) {
+    double x, y;
+    two_product(p[k], q[k], x, y);
+    grow(e, m, y);
+    ++m;
+    grow(e, m, x);
+    ++m;
+  }
+  return expansion_sign(e, m);
+}
 
 // Sign of sum_k p[k] q[k] for n <= 8 terms (a plane evaluated at a point, or
 // the difference of two planes there: the depth order of two sources).
@@ -192,19 +217,8 @@ EDP_HD inline int dot_sign(const double *p, const double *q, int n, int *stage =
     if (stage) *stage = kBinary64;
     return sign_of(s64);
   }
-  // Exact stage: every product as a two-component expansion, all grown into one.
-  double e[16];
-  int m = 0;
-  for (int k = 0; k < n; ++k) {
-    double x, y;
-    two_product(p[k], q[k], x, y);
-    grow(e, m, y);
-    ++m;
-    grow(e, m, x);
-    ++m;
-  }
   if (stage) *stage = kExact;
-  return expansion_sign(e, m);
+  return dot_sign_exact(p, q, n);
 }
 
 }  // namespace pred
