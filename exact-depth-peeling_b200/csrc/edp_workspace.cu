@@ -263,10 +263,12 @@ cudaError_t allocate_event(edp_peeler *p) {
 cudaError_t allocate_device(edp_peeler *p) {
   Dev &d = p->d;
   const int64_t n = d.n, F = d.cap.frontier, R = d.cap.regions, E = d.cap.vertices;
-  // Live clipping pieces end as visible (at most R) or hidden (at most F)
-  // pieces, so R + F slots hold every round's queue.
+  // Live clipping pieces end as visible (at most R) or hidden pieces, so
+  // R + F slots hold every round's queue.  The hidden pool also holds the
+  // pieces of targets that end up hidden whole (dropped when the layer
+  // finishes), so it takes R + F slots too.
   d.work_cap = int(std::min<int64_t>(R + F, (int64_t(1) << 31) - 1));
-  d.hidden_cap = int(F);
+  d.hidden_cap = d.work_cap;
   EDP_CHECK(allocate_shared(p));
   EDP_CHECK(alloc(p, &d.contour_lo, n));
   EDP_CHECK(alloc(p, &d.contour_hi, n));
@@ -284,9 +286,9 @@ cudaError_t allocate_device(edp_peeler *p) {
     EDP_CHECK(alloc(p, &d.work_target[k], d.work_cap));
     EDP_CHECK(alloc(p, &d.work_cursor[k], d.work_cap));
   }
-  EDP_CHECK(alloc(p, &d.hid_v, F * kMaxVertices));
-  EDP_CHECK(alloc(p, &d.hid_n, F));
-  EDP_CHECK(alloc(p, &d.hid_target, F));
+  EDP_CHECK(alloc(p, &d.hid_v, int64_t(d.hidden_cap) * kMaxVertices));
+  EDP_CHECK(alloc(p, &d.hid_n, d.hidden_cap));
+  EDP_CHECK(alloc(p, &d.hid_target, d.hidden_cap));
   EDP_CHECK(alloc(p, &d.target_visible, F));
   EDP_CHECK(alloc(p, &d.target_hidden, F));
   EDP_CHECK(alloc(p, &d.stats, 3 * d.cap.layers));

@@ -73,11 +73,14 @@ def tune(make, space=SPACE, replays=5, log=None):
     best_ms, expected = trial(make, best, replays, flush)
     default_ms = best_ms
     trials = [{"knobs": dict(best), "ms": best_ms}]
+    tried = {tuple(sorted(best.items()))}
     for knob, values in space.items():
         for value in values:
-            if value == best[knob]:
-                continue
             knobs = dict(best, **{knob: value})
+            key = tuple(sorted(knobs.items()))
+            if key in tried:
+                continue
+            tried.add(key)
             ms, counts = trial(make, knobs, replays, flush)
             trials.append({"knobs": knobs, "ms": ms})
             if log:
