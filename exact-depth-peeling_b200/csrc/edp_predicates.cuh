@@ -78,7 +78,7 @@ EDP_HD inline int expansion_sign(const double *e, int n) {
 // growing one expansion by all twelve components keeps the sum exact.  Out
 // of line: it is rare, and its expansion would otherwise take registers
 // from every caller.
-EDP_HD EDP_COLD int orient2d_exact(double ax, double ay, double bx, double by, double cx,
+EDP_HD inline EDP_COLD int orient2d_exact(double ax, double ay, double bx, double by, double cx,
                                    double cy) {
   double e[12];
   int n = 0;
@@ -161,7 +161,7 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
 
 // Exact stage of dot_sign: every product as a two-component expansion, all
 // grown into one (out of line, as orient2d_exact).
-EDP_HD EDP_COLD int dot_sign_exact(const double *p, const double *q, int n) {
+EDP_HD inline EDP_COLD int dot_sign_exact(const double *p, const double *q, int n) {
   double e[16];
   int m = 0;
   for (int k = 0; k < n; ++k) {
