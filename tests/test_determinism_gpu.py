@@ -1,0 +1,56 @@
+"""Replays of one graph give the same extraction as sets: atomic appends
+order the output polygons and triangles differently from one replay to the
+next (as in the reference), but the polygons (source, layer, vertices) and
+the triangles are the same, and so are the counts the tests check."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+
+
+def polygon_set(p):
+    info = p.read_status()
+    k = info["polygons"]
+    n = p.output.sizes[:k].cpu().numpy()
+    v = p.output.vertices[:k].cpu().numpy()
+    src = p.output_sources[:k].cpu().numpy()
+    lay = p.output_layers[:k].cpu().numpy()
+    rows = []
+    for i in range(k):
+        ring = v[i, : n[i]]
+        start = np.lexsort((ring[:, 1], ring[:, 0]))[0]  # a canonical first vertex
+        rows.append((int(src[i]), int(lay[i]), tuple(np.roll(ring, -start, axis=0).ravel())))
+    return sorted(rows), info
+
+
+def triangle_set(p, count):
+    uv = p.triangles_uv[:count].cpu().numpy().reshape(count, -1)
+    key = np.concatenate([uv, p.triangle_sources[:count].cpu().numpy()[:, None],
+                          p.triangle_layers[:count].cpu().numpy()[:, None]], axis=1)
+    return key[np.lexsort(key.T[::-1])]
+
+
+@pytest.mark.parametrize("config", ["icospheres-2560", "knot-65536"])
+def test_replays_give_the_same_sets(config):
+    from peel_b200 import scenes
+    from peel_b200.sizing import fit_event_capacities
+
+    p, _ = fit_event_capacities(scenes.to_device(scenes.CONFIGS[config]()))
+    p.run()
+    first, info1 = polygon_set(p)
+    tri1 = triangle_set(p, info1["triangles"])
+    p.run()
+    second, info2 = polygon_set(p)
+    tri2 = triangle_set(p, info2["triangles"])
+    for key in ("polygons", "triangles", "layers", "splits", "rounds", "ray_groups"):
+        assert info1[key] == info2[key], key
+    assert first == second
+    np.testing.assert_array_equal(tri1, tri2)
