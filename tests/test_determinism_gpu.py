@@ -1,7 +1,7 @@
 """Replays of one graph give the same extraction as sets: atomic appends
 order the output polygons and triangles differently from one replay to the
 next (as in the reference), but the polygons (source, layer, vertices) and
-the triangles are the same, and so are the counts the tests check."""
+the triangles are the same."""
 
 import numpy as np
 import pytest
@@ -50,7 +50,10 @@ def test_replays_give_the_same_sets(config):
     p.run()
     second, info2 = polygon_set(p)
     tri2 = triangle_set(p, info2["triangles"])
-    for key in ("polygons", "triangles", "layers", "splits", "rounds", "ray_groups"):
+    # The rank stage's counters (ray groups, hits) follow the representative
+    # each component gets, which is its first polygon in output order: they
+    # may vary, the ranks may not.
+    for key in ("polygons", "triangles", "layers", "splits", "rounds"):
         assert info1[key] == info2[key], key
     assert first == second
     np.testing.assert_array_equal(tri1, tri2)
