@@ -273,6 +273,9 @@ struct Dev {
   int workers, pieces;              // clipping threads; pieces one target may hold
   unsigned long long inner_handle;  // cudaGraphConditionalHandle of the clipping rounds
   int use_inner;
+  // Host-side: a second stream of the workspace, on which conditional node
+  // bodies are recorded while the workspace stream captures.
+  cudaStream_t aux_stream;
 };
 
 // Polygon edge `edge` of source `source` is a contour: every edge of a
@@ -324,6 +327,9 @@ namespace edp {
 // calls note_launch), used to report how many kernels a captured graph runs.
 void note_launch();
 int64_t launch_count();
+// Takes back n noted launches (kernels recorded in a conditional IF body that
+// an ordinary replay skips).
+void forget_launches(int64_t n);
 
 // Stage marks.  While a workspace captures its own graph, `events` holds
 // EDP_STAGE_COUNT + 1 timing events; stage_mark(-1, st) records the start

@@ -445,6 +445,7 @@ thread_local cudaEvent_t *g_marks = nullptr;
 thread_local int g_next_mark = 0;  // stages marked so far in this capture
 }
 void note_launch() { ++g_launches; }
+void forget_launches(int64_t n) { g_launches -= n; }
 int64_t launch_count() { return g_launches; }
 
 void set_stage_marks(cudaEvent_t *events) {

@@ -749,6 +749,12 @@ __global__ void k_group_sizes(Dev d) {
   if (__any_sync(0xffffffffu, large) && (threadIdx.x & 31) == 0) d.sc[kSortHits] = d.sc[kLiveHits];
 }
 
+// The condition of the global hit passes: some group is too deep for
+// k_group_sort.
+__global__ void k_sort_switch(Dev d, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, d.sc[kSortHits] != 0 ? 1u : 0u);
+}
+
 // Place each hit in its group's range (group_offsets is the scan of
 // group_counts); the order inside a group is fixed by k_group_sort.
 __global__ void k_hit_place(Dev d) {
@@ -1093,14 +1099,53 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   k_group_sizes<<<blocks(R), kBlock, 0, st>>>(d);
   note_launch();
   // Global passes: over all hits when some group is large, else over none.
-  const int pass_bits[3] = {bits_for(d.n), 64, bits_for(R)};
-  for (int stage = 0; stage < 3; ++stage) {
-    k_hit_keys<<<blocks(d.cap.hits), kBlock, 0, st>>>(d, stage);
+  // In a captured graph they sit in a conditional IF node, so an extraction
+  // whose groups all sort in k_group_sort launches none of their 40-odd
+  // kernels; run eagerly, they take their count (zero) from the device.
+  cudaStream_t radix = st;
+  const bool branch = d.use_handle && d.aux_stream;
+  if (branch) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    EDP_CHECK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphConditionalHandle handle;
+    EDP_CHECK(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+    k_sort_switch<<<1, 1, 0, st>>>(d, handle);
     note_launch();
-    EDP_CHECK(sort_pairs_u64(reinterpret_cast<uint64_t *>(d.hkeys),
-                             reinterpret_cast<uint64_t *>(d.hkeys_tmp), d.hit_ids, d.hit_ids_tmp,
-                             d.sc + kSortHits, d.cap.hits, pass_bits[stage], s, st));
+    EDP_CHECK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    EDP_CHECK(cudaGraphAddNode(&node, g, deps, ndeps, &params));
+    EDP_CHECK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    EDP_CHECK(cudaStreamBeginCaptureToGraph(d.aux_stream, params.conditional.phGraph_out[0],
+                                            nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    radix = d.aux_stream;
   }
+  const int pass_bits[3] = {bits_for(d.n), 64, bits_for(R)};
+  const int64_t body_first = launch_count();
+  cudaError_t sorted = cudaSuccess;
+  for (int stage = 0; stage < 3 && sorted == cudaSuccess; ++stage) {
+    k_hit_keys<<<blocks(d.cap.hits), kBlock, 0, radix>>>(d, stage);
+    note_launch();
+    sorted = sort_pairs_u64(reinterpret_cast<uint64_t *>(d.hkeys),
+                            reinterpret_cast<uint64_t *>(d.hkeys_tmp), d.hit_ids, d.hit_ids_tmp,
+                            d.sc + kSortHits, d.cap.hits, pass_bits[stage], s, radix);
+  }
+  if (branch) {
+    cudaGraph_t body = nullptr;
+    cudaError_t end = cudaStreamEndCapture(d.aux_stream, &body);
+    EDP_CHECK(sorted);
+    EDP_CHECK(end);
+    forget_launches(launch_count() - body_first);
+  }
+  EDP_CHECK(sorted);
   EDP_CHECK(cudaMemsetAsync(d.group_fill, 0, sizeof(int) * R, st));
   k_hit_place<<<blocks(d.cap.hits), kBlock, 0, st>>>(d);
   note_launch();

@@ -467,12 +467,15 @@ int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, i
   d.propagate_ranks = o.propagate_ranks != 0;
   d.merge_regions = o.merge_regions != 0;
   d.predicates = EDP_PREDICATES_FILTERED;
+  d.aux_stream = nullptr;
   d.step_budget = 48;
   d.subdivide_blocks = 8;
   d.heavy_noding_work = 1024;
   d.clip_budget = 32;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->round_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) d.aux_stream = p->round_stream;
   if (e == cudaSuccess) e = allocate_event(p);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
