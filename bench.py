@@ -385,7 +385,7 @@ def time_replays(p, steps, flush):
 
 
 def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_leg,
-                   audit_samples, compare_forms=False):
+                   audit_samples, compare_forms=False, compare_pools=False):
     """Time one single-mesh configuration; returns its measurement dict.
 
     Device time: `steps` replays of the captured extraction after
@@ -552,6 +552,30 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
             "polygons", "vertices_measured", "unexplained_vertices", "max_abs_error",
             "scene_extent", "max_rel_error")}
         result["vertex_error_max"] = report["max_rel_error"]
+    if compare_pools:
+        # Pool sizing: the trained network's pools against the worst-case
+        # sizing (EventCapacities.for_mesh) and the fitted pools timed above.
+        from peel_b200 import EventCapacities, learned
+
+        sized, learned_cap, fell_back = learned.peel(arrays)
+        sized.set_tuning(**knobs)
+        sized.capture()
+        for _ in range(args.warmup):
+            sized.run()
+        learned_ms = time_replays(sized, max(5, steps // 4), flush)
+        learned_bytes = learned.workspace_bytes(sized)
+        same = sized.read_status()["triangles"] == check["triangles"]
+        del sized
+        worst = EventPeeler(*arrays, capacities=EventCapacities.for_mesh(len(faces)))
+        worst_bytes = learned.workspace_bytes(worst)
+        del worst
+        result["pool_sizing"] = {
+            "learned_bytes": learned_bytes, "worst_case_bytes": worst_bytes,
+            "learned_over_worst_case": learned_bytes / worst_bytes, "fell_back": fell_back,
+            "learned_ms": learned_ms, "same_triangles": bool(same),
+            "learned_capacities": vars(learned_cap),
+            "network": "16-64-64-3 perceptron, BF16 weights on the tensor cores "
+                       "(peel_b200/pool_sizing.json)"}
     if compare_forms:
         # The same extraction under the other predicate forms: the
         # reference's plain binary64 signs (the comparator of the filtered
@@ -600,7 +624,7 @@ def run_ours(args, rank, world, local_rank):
     if args.config == "knot-65536" and not quick:
         second = measure_config(SECOND_CONFIG, args, rank, world, local_rank,
                                 max(5, args.steps // 5), 3, world == 1, 300,
-                                compare_forms=True)
+                                compare_forms=True, compare_pools=True)
         if second is not None:
             extra[SECOND_CONFIG] = second
     if rank != 0:

@@ -9,7 +9,8 @@
 //   2  filtered and counted: as 1, and every call is tallied by predicate
 //      class and deciding stage into Dev::pred_counts;
 //   3  filtered from binary64: the same exact signs with the binary32 stage
-//      skipped (the binary64 filter first, then expansion arithmetic).
+//      skipped (orientation through orient2d_lean, the binary64 filter as one
+//      bound test, then expansion arithmetic).
 // Constructions (intersection points, clip parameters, depths stored for the
 // hit sort's radix fallback) stay binary64 in every form.
 #pragma once
@@ -68,8 +69,10 @@ template <int F>
 __device__ inline int side_sign(V2 a, V2 b, V2 c, int &stage) {
   if constexpr (F == 0) {
     return sign_of(cross(a, b, c));
+  } else if constexpr (F == 3) {
+    return pred::orient2d_lean(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
   } else {
-    return pred::orient2d(a.x, a.y, b.x, b.y, c.x, c.y, &stage, F != 3);
+    return pred::orient2d(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
   }
 }
 

@@ -70,6 +70,7 @@ struct Segments {
   const int *ids;
   const V2 *a, *b, *near;
   const int2 *near_src;  // the sources whose planes give `near`
+  const V2 *near_mag;    // their |a x| + |b y| + |c| at the ends
   const Plane *scores;
 };
 
@@ -90,14 +91,17 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
   const int lane = threadIdx.x & 31;
   const bool mine = lane < n;
   const int width = lane_width(n);
-  V2 ca = v2(0.0, 0.0), cb = ca, cn = ca;
+  V2 ca = v2(0.0, 0.0), cb = ca, cn = ca, cm = ca;
   int2 cs = make_int2(0, 0);
   if ((batch >> lane) & 1u) {
     const int c = __ldg(&g.ids[first + lane]);
     ca = g.a[c];
     cb = g.b[c];
     cn = g.near[c];
-    if constexpr (F != 0) cs = g.near_src[c];
+    if constexpr (F != 0) {
+      cs = g.near_src[c];
+      cm = g.near_mag[c];
+    }
   }
   while (batch) {
     const int k = __ffs(int(batch)) - 1;
@@ -122,12 +126,31 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
       szb = sign_of(zb);
     } else {
       // The patch's depth plane against the plane of the source that gives
-      // the segment its near depth, both at the segment's ends: exact, and
-      // zero when that source is the patch's own.
+      // the segment its near depth, at the segment's ends.  Each binary64
+      // evaluation is within 3.01 u of its terms' magnitudes (two products,
+      // two sums), so a difference above 4 u of both magnitudes has its sign;
+      // otherwise the two planes are compared exactly (zero when the
+      // source is the patch's own).
       int stage_b = 0;
-      const int sa = __shfl_sync(kFull, cs.x, k), sb = __shfl_sync(kFull, cs.y, k);
-      sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
-      szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
+      const V2 mag = shfl(cm, k);
+      const double bound_a = 4.0 * pred::kU64 *
+          (fabs(sc.a * a.x) + fabs(sc.b * a.y) + fabs(sc.c) + mag.x);
+      const double bound_b = 4.0 * pred::kU64 *
+          (fabs(sc.a * b.x) + fabs(sc.b * b.y) + fabs(sc.c) + mag.y);
+      if (fabs(za) > bound_a) {
+        sza = sign_of(za);
+        stage = pred::kBinary64;
+      } else {
+        const int sa = __shfl_sync(kFull, cs.x, k);
+        sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
+      }
+      if (fabs(zb) > bound_b) {
+        szb = sign_of(zb);
+        stage_b = pred::kBinary64;
+      } else {
+        const int sb = __shfl_sync(kFull, cs.y, k);
+        szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
+      }
       if constexpr (F == 2) {
         if (lane == 0) {  // the same test on every lane: count it once
           tally.depth.add(stage);
@@ -319,7 +342,8 @@ __global__ void __launch_bounds__(kBlock, F == 0 ? 5 : 4) k_subdivide(Dev d) {
   const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
   const int leaves = *d.seg_tree.size;
   const int next_lane = lane + 1;
-  const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near, d.seg_near_src, d.scores};
+  const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near, d.seg_near_src,
+                      d.seg_near_mag, d.scores};
   const Frontier next{d.fv[par ^ 1], d.fn[par ^ 1], d.fsrc[par ^ 1], d.fcur[par ^ 1],
                       &d.status[kNextResidual], d.status, d.cap.frontier};
   long long visits = 0, tests = 0, splits = 0;  // lane 0's tallies

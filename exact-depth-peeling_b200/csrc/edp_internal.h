@@ -179,6 +179,7 @@ struct Dev {
   // depth b) and boxes; the contour hierarchy is built over these.
   V2 *seg_a, *seg_b, *seg_near;
   int2 *seg_near_src;  // the sources whose depth planes give seg_near (exact depth tests)
+  V2 *seg_near_mag;    // per end, |a x| + |b y| + |c| of that plane: the depth's error scale
   float4 *seg_lo, *seg_hi;
   int *seg_table, *seg_min, *seg_slot;
   int seg_mask;

@@ -157,6 +157,24 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
   return orient2d_exact(ax, ay, bx, by, cx, cy);
 }
 
+// orient2d without the binary32 stage and without sign-case branches:
+// Shewchuk's first binary64 filter as one bound test, then the exact stage.
+// Same sign as orient2d (inputs whose products underflow excepted, as for
+// Shewchuk's filter).
+EDP_HD inline int orient2d_lean(double ax, double ay, double bx, double by, double cx,
+                                double cy, int *stage = nullptr) {
+  const double detleft = (ax - cx) * (by - cy);
+  const double detright = (ay - cy) * (bx - cx);
+  const double det = detleft - detright;
+  const double bound = (3.0 + 16.0 * kU64) * kU64 * (fabs(detleft) + fabs(detright));
+  if (det > bound || -det > bound || bound == 0.0) {
+    if (stage) *stage = kBinary64;
+    return sign_of(det);
+  }
+  if (stage) *stage = kExact;
+  return orient2d_exact(ax, ay, bx, by, cx, cy);
+}
+
 // ---------------------------------------------------------------- linear forms
 
 // Exact stage of dot_sign: every product as a two-component expansion, all

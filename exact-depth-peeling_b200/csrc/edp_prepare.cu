@@ -356,7 +356,17 @@ __global__ void k_segment_compact(Dev d) {
     d.seg_a[c] = a;
     d.seg_b[c] = b;
     d.seg_near[c] = v2(za, zb);
-    d.seg_near_src[c] = make_int2(d.seg_srca[slot], d.seg_srcb[slot]);
+    // Every group has a member attaining each minimum (the same binary64
+    // expression is evaluated again); the representative's own source
+    // stands in should none have been recorded.
+    const int own = int(i / kSourceVertices);
+    int2 near_src = make_int2(d.seg_srca[slot], d.seg_srcb[slot]);
+    if (near_src.x < 0 || near_src.x >= d.n) near_src.x = own;
+    if (near_src.y < 0 || near_src.y >= d.n) near_src.y = own;
+    d.seg_near_src[c] = near_src;
+    const Plane pa = d.scores[near_src.x], pb = d.scores[near_src.y];
+    d.seg_near_mag[c] = v2(fabs(pa.a * a.x) + fabs(pa.b * a.y) + fabs(pa.c),
+                           fabs(pb.a * b.x) + fabs(pb.b * b.y) + fabs(pb.c));
     d.seg_lo[c] = make_float4(float(fmin(a.x, b.x) - 2.0e-7), float(fmin(a.y, b.y) - 2.0e-7),
                               float(fmin(za, zb) - pz), 0.f);
     d.seg_hi[c] = make_float4(float(fmax(a.x, b.x) + 2.0e-7), float(fmax(a.y, b.y) + 2.0e-7),

@@ -185,6 +185,7 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.seg_b, S));
   EDP_CHECK(alloc(p, &d.seg_near, S));
   EDP_CHECK(alloc(p, &d.seg_near_src, S));
+  EDP_CHECK(alloc(p, &d.seg_near_mag, S));
   EDP_CHECK(alloc(p, &d.seg_lo, S));
   EDP_CHECK(alloc(p, &d.seg_hi, S));
   EDP_CHECK(alloc(p, &d.seg_slot, S));

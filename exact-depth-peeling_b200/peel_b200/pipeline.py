@@ -93,7 +93,9 @@ class PeelStream:
 
 
 def as_numpy(result):
-    """{name: numpy array} of a collected result (after its event)."""
+    """(status, {name: numpy array}) of a collected result: waits for its
+    copy and copies the arrays out of the pinned buffers, which the stream
+    reuses ``depth`` submissions later."""
     status, views, done = result
     done.synchronize()
-    return status, {name: np.asarray(v.numpy()) for name, v in views.items()}
+    return status, {name: v.numpy().copy() for name, v in views.items()}

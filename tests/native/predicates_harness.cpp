@@ -15,3 +15,10 @@ extern "C" void dot_sign_batch(const double *p, const double *q, int terms, long
   for (long i = 0; i < count; ++i)
     signs[i] = edp::pred::dot_sign(p + terms * i, q + terms * i, terms, &stages[i]);
 }
+
+extern "C" void orient2d_lean_batch(const double *points, long count, int *signs, int *stages) {
+  for (long i = 0; i < count; ++i) {
+    const double *p = points + 6 * i;
+    signs[i] = edp::pred::orient2d_lean(p[0], p[1], p[2], p[3], p[4], p[5], &stages[i]);
+  }
+}

@@ -27,6 +27,7 @@ def lib(tmp_path_factory):
     handle = ctypes.CDLL(str(out))
     P = ctypes.c_void_p
     handle.orient2d_batch.argtypes = [P, ctypes.c_long, P, P]
+    handle.orient2d_lean_batch.argtypes = [P, ctypes.c_long, P, P]
     handle.dot_sign_batch.argtypes = [P, P, ctypes.c_int, ctypes.c_long, P, P]
     return handle
 
@@ -151,3 +152,29 @@ def test_every_term_count(lib, terms):
     q[:, -1] = -(p[:, :-1] * q[:, :-1]).sum(axis=1) / p[:, -1] if terms > 1 else q[:, -1]
     signs, _ = dots(lib, p, q)
     np.testing.assert_array_equal(signs, [exact_dot(a, b) for a, b in zip(p, q)])
+
+
+def test_lean_filter_gives_the_same_signs(lib):
+    """orient2d_lean (the binary64 filter as one bound test, then exact) agrees
+    with the exact sign on random, nearly collinear and exactly collinear
+    points, and escalates only where the filter cannot certify."""
+    rng = np.random.default_rng(7)
+    a = rng.uniform(-1, 1, size=(500, 2))
+    b = rng.uniform(-1, 1, size=(500, 2))
+    t_ = rng.uniform(-2, 2, size=(500, 1))
+    on_line = a + t_ * (b - a)
+    near = on_line + rng.normal(scale=1e-15, size=on_line.shape)
+    for c in (rng.uniform(-1, 1, size=(500, 2)), on_line, near):
+        rows = np.hstack([a, b, c])
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        signs = np.zeros(len(rows), dtype=np.int32)
+        stages = np.zeros(len(rows), dtype=np.int32)
+        lib.orient2d_lean_batch(rows.ctypes.data, len(rows), signs.ctypes.data,
+                                stages.ctypes.data)
+        np.testing.assert_array_equal(signs, [exact_orient(r) for r in rows])
+        assert set(stages.tolist()) <= {BINARY64, EXACT}
+    grid = np.array([[0.0, 0.0, 1.0, 1.0, 0.5, 0.5], [0.0, 0.0, 0.0, 0.0, 1.0, 2.0]])
+    signs = np.zeros(2, dtype=np.int32)
+    stages = np.zeros(2, dtype=np.int32)
+    lib.orient2d_lean_batch(grid.ctypes.data, 2, signs.ctypes.data, stages.ctypes.data)
+    assert signs.tolist() == [0, 0]
