@@ -614,6 +614,33 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
 SECOND_CONFIG = "primitives-720k"  # the metric's other mesh (720K faces)
 
 
+def measure_device_peeler(args, local_rank, config="icospheres-2560", steps=20):
+    """The iterative-clipping route (DevicePeeler) on the nested icospheres:
+    device ms per mesh, its workspace, and what per-worker pools of the
+    reference's defaults would take (workers x pieces_per_worker x 3
+    polygons of 32 double2 vertices and a count)."""
+    import torch
+
+    from peel_b200 import Capacities, DevicePeeler, learned, scenes
+
+    device = torch.device("cuda", local_rank)
+    host = scenes.CONFIGS[config]()
+    arrays = scenes.to_device(host, device)
+    cap = Capacities.for_mesh(len(host[1]))
+    p = DevicePeeler(*arrays, capacities=cap)
+    p.capture()
+    for _ in range(args.warmup):
+        p.run()
+    info = p.read_status()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    ms = time_replays(p, steps, flush)
+    return {"config": config, "ms_per_mesh": ms, "steps": steps,
+            "output": {k: info[k] for k in ("polygons", "triangles", "layers")},
+            "workspace_bytes": learned.workspace_bytes(p),
+            "per_worker_pool_bytes_at_reference_defaults":
+                cap.workers * cap.pieces_per_worker * 3 * (32 * 16 + 4)}
+
+
 def run_ours(args, rank, world, local_rank):
     quick = args.quick
     first = measure_config(args.config, args, rank, world, local_rank, args.steps,
@@ -627,6 +654,7 @@ def run_ours(args, rank, world, local_rank):
                                 compare_forms=True, compare_pools=True)
         if second is not None:
             extra[SECOND_CONFIG] = second
+    device_peeler = None if quick else measure_device_peeler(args, local_rank)
     if rank != 0:
         return
     line = {
@@ -638,6 +666,8 @@ def run_ours(args, rank, world, local_rank):
     line.update({k: v for k, v in first.items() if k not in ("value", "ms_per_step", "steps")})
     if extra:
         line["configs"] = extra
+    if device_peeler:
+        line["device_peeler"] = device_peeler
     print(json.dumps(line), flush=True)
 
 
