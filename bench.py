@@ -33,7 +33,7 @@ UNIT = "ms/mesh"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 REFERENCE_BUDGET_S = 60.0  # CPU seconds of timed extractions in the reference arm
-DEFAULT_FORM = "filtered"  # the predicate form of EventPeeler's default
+DEFAULT_FORM = "filtered64"  # the predicate form of EventPeeler's default
 
 
 DESCRIPTIONS = {

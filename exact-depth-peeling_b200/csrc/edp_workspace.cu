@@ -467,7 +467,7 @@ int edp_event_create(const double *vertices, int64_t nv, const int32_t *faces, i
   d.share_regions = o.share_regions != 0;
   d.propagate_ranks = o.propagate_ranks != 0;
   d.merge_regions = o.merge_regions != 0;
-  d.predicates = EDP_PREDICATES_FILTERED;
+  d.predicates = EDP_PREDICATES_FILTERED64;
   d.aux_stream = nullptr;
   d.step_budget = 48;
   d.subdivide_blocks = 8;
@@ -523,7 +523,7 @@ int edp_device_create(const double *vertices, int64_t nv, const int32_t *faces, 
   d.all_layers = layers == 0;
   d.workers = int(c.workers);
   d.pieces = int(c.pieces_per_worker);
-  d.predicates = EDP_PREDICATES_FILTERED;
+  d.predicates = EDP_PREDICATES_FILTERED64;
   d.step_budget = 48;
   d.subdivide_blocks = 8;
   d.heavy_noding_work = 1024;

@@ -55,15 +55,17 @@ class EventPeeler(_Peeler):
     Inputs must have resolved surface intersections.
 
     ``predicates`` (not in the reference, whose kernels are plain binary64)
-    selects the sign predicates: "filtered" (exact signs through binary32 and
-    binary64 filters and expansion arithmetic), "binary64" (the reference's
-    plain expressions) or "counted" (filtered, with per-class tallies of the
-    deciding stage, read by ``predicate_counts()``).
+    selects the sign predicates: "filtered64" (the default: exact signs
+    through a binary64 filter and expansion arithmetic), "filtered" (exact
+    signs through binary32, then binary64 filters, then expansions),
+    "binary64" (the reference's plain expressions) or "counted" ("filtered",
+    with per-class tallies of the deciding stage, read by
+    ``predicate_counts()``).
     """
 
     def __init__(self, vertices, faces, camera, settings, *, capacities=None, layers=0,
                  share_regions=True, propagate_ranks=True, merge_regions=False,
-                 predicates="filtered"):
+                 predicates="filtered64"):
         import torch
 
         self.device = _check_inputs(vertices, faces, camera, settings)

@@ -285,7 +285,7 @@ class DevicePeeler(_Peeler):
     """
 
     def __init__(self, vertices, faces, camera, settings, *, capacities=None, layers=0,
-                 predicates="filtered"):
+                 predicates="filtered64"):
         import torch
 
         self.device = _check_inputs(vertices, faces, camera, settings)

@@ -145,7 +145,8 @@ int edp_run_stage(edp_peeler *p, int32_t stage);
  * the reference's plain binary64 expressions, or exact signs through
  * escalating filters (binary32 with a static error bound, then binary64, then
  * exact expansion arithmetic), optionally tallied per class and deciding
- * stage.  Workspaces start FILTERED.  Constructions stay binary64. */
+ * stage.  Workspaces start FILTERED64 (the faster exact form on a B200).
+ * Constructions stay binary64. */
 enum edp_predicates {
   EDP_PREDICATES_BINARY64 = 0,
   EDP_PREDICATES_FILTERED = 1,   /* binary32 filter, binary64 filter, exact */

@@ -39,7 +39,8 @@ def test_every_form_matches_the_oracle(name, form):
 
 def test_counted_tallies_every_class():
     """Nested icospheres: each class of the contour route is evaluated, most
-    calls are decided in binary32, and the forms give the same regions."""
+    calls are decided by the first filter, and the forms give the same
+    regions."""
     from peel_b200 import EventPeeler, scenes
 
     arrays = scenes.to_device(scenes.nested_icospheres())
@@ -49,7 +50,10 @@ def test_counted_tallies_every_class():
     for cls in ("side", "segment", "depth", "contain", "order"):
         total = sum(counts[cls].values())
         assert total > 0, (cls, counts)
-        assert counts[cls]["binary32"] >= 0.5 * total, (cls, counts)
+        # The depth test's filter is a binary64 bound on the two planes'
+        # magnitudes; the others start in binary32.
+        decided = counts[cls]["binary32"] + (counts[cls]["binary64"] if cls == "depth" else 0)
+        assert decided >= 0.5 * total, (cls, counts)
     assert sum(counts["clip"].values()) == 0
     plain = EventPeeler(*arrays, predicates="binary64")
     plain.run()
@@ -60,9 +64,9 @@ def test_counted_tallies_every_class():
     labels = range(arrays[1].shape[0])
     parity.assert_areas(parity.gpu_areas(parity.polygons(counted), labels),
                         parity.gpu_areas(parity.polygons(plain), labels))
-    filtered = EventPeeler(*arrays)
-    filtered.run()
-    assert sum(sum(v.values()) for v in filtered.predicate_counts().values()) == 0
+    uncounted = EventPeeler(*arrays)
+    uncounted.run()
+    assert sum(sum(v.values()) for v in uncounted.predicate_counts().values()) == 0
 
 
 def test_exact_degeneracy_is_never_decided_in_binary32():
