@@ -366,6 +366,22 @@ def run_batched(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def stage_medians(p, replays, flush):
+    """Per-stage device ms from the graph's own timing events (each replay
+    records the end of every stage, so the stages sum to the replay): median
+    over `replays` L2-flushed replays."""
+    import torch
+
+    samples = {}
+    for _ in range(replays):
+        with torch.cuda.stream(p.stream):
+            flush.zero_()
+        p.run()
+        for name, ms in p.stage_times().items():
+            samples.setdefault(name, []).append(ms)
+    return {name: statistics.median(v) for name, v in samples.items()}
+
+
 def time_replays(p, steps, flush):
     """Mean device ms of `steps` replays of p's graph, each after an L2 flush
     (CUDA events on the workspace stream)."""
@@ -411,10 +427,15 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
     # The autotuner's coordinate search over the work-distribution knobs
     # (same outputs under every choice); the timed replays use its choice.
     from peel_b200 import EventPeeler
-    from peel_b200.autotune import tune
+    from peel_b200.autotune import SPACE, tune
 
-    knobs, default_ms, tuned_ms, trials = tune(
-        lambda: EventPeeler(*arrays, capacities=capacities), replays=5)
+    if args.quick:  # profiler runs keep the default knobs
+        knobs = {k: v for k, v in p.tuning().items() if k in SPACE}
+        default_ms = tuned_ms = None
+        trials = []
+    else:
+        knobs, default_ms, tuned_ms, trials = tune(
+            lambda: EventPeeler(*arrays, capacities=capacities), replays=5)
     p.set_tuning(**knobs)
     p.capture()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
@@ -442,16 +463,7 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
     ms_per_mesh = whole_job_ms_per_mesh(total, steps, world)
     check = p.read_status()
 
-    # Per-stage device time from the graph's own timing events: each replay
-    # records the end of every stage, so the stages sum to the replay.
-    samples = {}
-    for _ in range(max(5, min(steps, 21))):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        p.run()
-        for name, ms in p.stage_times().items():
-            samples.setdefault(name, []).append(ms)
-    stage_ms = {name: statistics.median(v) for name, v in samples.items()}
+    stage_ms = stage_medians(p, max(5, min(steps, 21)), flush)
 
     pinned = [torch.as_tensor(a).pin_memory() for a in host]
     t_count = check["triangles"]
@@ -594,7 +606,8 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
             ms = time_replays(other, steps, flush)
             info = other.read_status()
             timed[form] = {"ms": ms, "output": {k: info[k] for k in ("polygons", "triangles",
-                                                                     "layers")}}
+                                                                     "layers")},
+                           "stages_ms": stage_medians(other, 7, flush)}
             del other
         counted, _ = fit_event_capacities(arrays, capacities, predicates="counted")
         counted.run()
@@ -679,7 +692,8 @@ def main():
     ap.add_argument("--config", default="knot-65536")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--quick", action="store_true",
-                    help="skip the CPU baseline and the end-to-end leg (for profiler runs)")
+                    help="skip the autotuner, the CPU baseline and the end-to-end leg "
+                         "(for profiler runs)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

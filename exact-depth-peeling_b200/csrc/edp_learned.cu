@@ -136,7 +136,10 @@ __global__ void k_tile_raw_clear(float *raw, int *totals) {
   }
 }
 
-// The sixteen features of each tile (one thread per tile).
+// The sixteen features of each tile (one thread per tile).  Counts are taken
+// per 4,096 faces of the mesh and lengths per sqrt(faces / 4,096), so that a
+// mesh ten times finer over the same shapes gives about the same features
+// (the network trained on 4K-64K faces then sizes larger meshes too).
 __global__ void k_tile_finish(const float *raw, const int *totals, int nf, float *features) {
   const int t = threadIdx.x + blockIdx.x * blockDim.x;
   if (t >= kTiles) return;
@@ -145,23 +148,25 @@ __global__ void k_tile_finish(const float *raw, const int *totals, int nf, float
   const float gmin = order_float(totals[1]), gmax = order_float(totals[2]);
   const float span = gmax > gmin ? gmax - gmin : 1.0f;
   const float count = r[0];
+  const float per = 4096.0f / float(nf > 0 ? nf : 1);  // counts per 4,096 faces
+  const float len = sqrtf(per);
   const float zlo = count > 0.0f ? (order_float(__float_as_int(r[8])) - gmin) / span : 1.0f;
   const float zhi = count > 0.0f ? (order_float(__float_as_int(r[9])) - gmin) / span : 0.0f;
   const float zmean = count > 0.0f ? (r[10] / count - gmin) / span : 0.5f;
   float *out = features + int64_t(kIn) * t;
-  out[0] = log1pf(count);
+  out[0] = log1pf(count * per);
   out[1] = log1pf(r[1] / tile_area);
   out[2] = log1pf(r[2] / tile_area);
-  out[3] = log1pf(r[3]);
-  out[4] = log1pf(r[4]);
-  out[5] = log1pf(r[5] / tile_side);
-  out[6] = log1pf(r[6]);
-  out[7] = log1pf(r[7]);
+  out[3] = log1pf(r[3] * per);
+  out[4] = log1pf(r[4] * per);
+  out[5] = log1pf(r[5] / tile_side * len);
+  out[6] = log1pf(r[6] * per);
+  out[7] = log1pf(r[7] * per);
   out[8] = zlo;
   out[9] = zhi;
   out[10] = zmean;
-  out[11] = log1pf(r[11]);
-  out[12] = log1pf(float(nf));
+  out[11] = log1pf(r[11] * per);
+  out[12] = count > 0.0f ? r[3] / count : 0.5f;  // front-facing share
   out[13] = log1pf(__int_as_float(totals[0]));
   out[14] = (float(t % kTileAxis) + 0.5f) * tile_side;
   out[15] = (float(t / kTileAxis) + 0.5f) * tile_side;

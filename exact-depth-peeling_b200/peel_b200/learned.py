@@ -13,7 +13,10 @@ features (``edp_tile_features``), and the sums size the pools:
 * hits = m_H * sum(F * L)  (a ray group holds at most one hit per layer)
 * layers = m_L * max(L)
 
-with margins m fixed from the training set.  An extraction that overflows a
+with margins m fixed from the training set, and none above the worst-case
+sizing.  Fragment and triangle counts are learned per 4,096 faces, with the
+count features scaled alike, so the network trained on 4K-64K-face meshes
+sizes finer meshes of the same kind.  An extraction that overflows a
 learned pool reruns with ``EventCapacities.for_mesh`` (``peel``), so the
 outputs never depend on the prediction; only the memory does.
 
@@ -46,6 +49,17 @@ TILE_AXIS, INPUTS, HIDDEN, OUTPUTS, PARAMS = 16, 16, 64, 3, 5443
 TILES = TILE_AXIS * TILE_AXIS
 SCRATCH = TILES * 12 + 4
 TARGETS = ("fragments", "triangles", "layers")
+PER_FACES = 4096  # fragment and triangle counts are learned per 4,096 faces
+FORMAT = "peel-b200-pool-sizing-v2"  # features and targets per PER_FACES faces
+
+
+def per_faces(counts, faces, inverse=False):
+    """Counts [tiles, 3] with fragments and triangles taken per PER_FACES
+    faces (or back, with `inverse`); layers are left as they are."""
+    out = np.array(counts, dtype=np.float64, copy=True)
+    scale = PER_FACES / max(int(faces), 1)
+    out[:, :2] = out[:, :2] / scale if inverse else out[:, :2] * scale
+    return out
 # Offsets of the parameter blocks (edp.h): W1, b1, W2, b2, W3, b3.
 SLICES = {"W1": (0, (HIDDEN, INPUTS)), "b1": (1024, (HIDDEN,)), "W2": (1088, (HIDDEN, HIDDEN)),
           "b2": (5184, (HIDDEN,)), "W3": (5248, (OUTPUTS, HIDDEN)), "b3": (5440, (OUTPUTS,))}
@@ -153,6 +167,10 @@ class PoolSizer:
         import torch
 
         data = json.loads(Path(path).read_text())
+        if data.get("format") != FORMAT:
+            raise ValueError(f"{path}: weights in format {data.get('format')!r}, "
+                             f"expected {FORMAT!r} (retrain with `python -m peel_b200.learned "
+                             "train`)")
         self.meta = data
         self.params = torch.tensor(data["params"], dtype=torch.float32, device=device)
         self.mean = torch.tensor(data["feature_mean"], dtype=torch.float32, device=device)
@@ -163,7 +181,7 @@ class PoolSizer:
         """[tiles, 3] predicted counts (host numpy)."""
         x = (tile_features(arrays) - self.mean) / self.std
         y = infer(self.params, x).double().cpu().numpy()
-        return np.expm1(np.clip(y, 0.0, 30.0))
+        return per_faces(np.expm1(np.clip(y, 0.0, 30.0)), arrays[1].shape[0], inverse=True)
 
     def capacities(self, arrays, scale=1.0):
         """EventCapacities for a mesh; `scale` multiplies the prediction (a
@@ -174,16 +192,16 @@ class PoolSizer:
 
 def capacities_from_counts(counts, margins, faces):
     """EventCapacities from per-tile counts [tiles, 3] (fragments, triangles,
-    layers) and the margins; the layer capacity never exceeds the worst
-    case's."""
+    layers) and the margins; no pool exceeds the worst-case sizing's."""
     base = EventCapacities.for_mesh(faces)
     fragments, triangles, layers = counts[:, 0], counts[:, 1], counts[:, 2]
     regions = int(margins["fragments"] * fragments.sum()) + 256
     tris = int(margins["triangles"] * triangles.sum()) + 1024
     hits = int(margins["hits"] * (fragments * np.maximum(layers, 1.0)).sum()) + 1024
     depth = int(margins["layers"] * layers.max(initial=1.0)) + 8
-    return replace(base, frontier=regions, regions=regions, hits=hits,
-                   vertices=tris + 2 * regions, triangles=tris, layers=min(base.layers, depth))
+    return replace(base, frontier=min(base.frontier, regions), regions=min(base.regions, regions),
+                   hits=min(base.hits, hits), vertices=min(base.vertices, tris + 2 * regions),
+                   triangles=min(base.triangles, tris), layers=min(base.layers, depth))
 
 
 OVERFLOW = 2 | 4 | 8 | 16 | 32 | 64 | 1024 | 2048  # pool-capacity bits of status[9]
@@ -242,8 +260,9 @@ def dataset(seeds, device="cuda", processes=None):
         p, _ = fit_event_capacities(arrays, headroom=1.0)
         info = p.read_status()  # raises on a failed extraction
         feats.append(tile_features(arrays).cpu().numpy())
-        targs.append(tile_targets(p))
-        assert targs[-1][:, 1].sum() == info["triangles"]
+        raw = tile_targets(p)
+        assert raw[:, 1].sum() == info["triangles"]
+        targs.append(per_faces(raw, len(host[1])))
         del p
     return np.stack(feats), np.stack(targs)
 
@@ -345,7 +364,7 @@ def main(argv=None):
     ratios = coverage_ratios(params, mean, std, features, targets)
     margins, distribution = margins_for(ratios)
     args.out.write_text(json.dumps({
-        "format": "peel-b200-pool-sizing-v1",
+        "format": FORMAT,
         "layout": "W1[64][16], b1[64], W2[64][64], b2[64], W3[3][64], b3[3]; weights applied "
                   "as BF16, float32 master values stored",
         "targets": ["log1p(" + name + " per tile)" for name in TARGETS],

@@ -56,6 +56,8 @@ def test_capacities_from_counts():
     assert cap.layers == int(1.25 * 4) + 8
     base = EventCapacities.for_mesh(65536)
     assert cap.regions < base.regions and cap.hits < base.hits
+    huge = learned.capacities_from_counts(counts * 1e6, margins, 65536)
+    assert (huge.regions, huge.hits, huge.triangles) == (base.regions, base.hits, base.triangles)
     few = np.zeros_like(counts)
     few[0] = [10.0, 30.0, 40.0]
     assert learned.capacities_from_counts(few, margins, 4).layers == EventCapacities.for_mesh(4).layers
@@ -70,3 +72,12 @@ def test_training_meshes_are_seeded_and_in_range():
         v, f, camera, settings = scenes.training_mesh(seed)
         assert 3000 <= len(f) <= 70000
         assert settings[4] == 1.0
+
+
+def test_counts_per_faces_round_trip():
+    from peel_b200 import learned
+
+    counts = np.array([[100.0, 300.0, 4.0], [0.0, 0.0, 0.0]])
+    scaled = learned.per_faces(counts, 8192)
+    assert scaled[0].tolist() == [50.0, 150.0, 4.0]
+    np.testing.assert_array_equal(learned.per_faces(scaled, 8192, inverse=True), counts)
