@@ -422,7 +422,8 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
     host = scenes.CONFIGS[config]()
     vertices, faces, camera, settings = host
     arrays = scenes.to_device(host, device)
-    p, capacities = fit_event_capacities(arrays)
+    form = args.predicates
+    p, capacities = fit_event_capacities(arrays, predicates=form)
     lib = _lib.load()
     # The autotuner's coordinate search over the work-distribution knobs
     # (same outputs under every choice); the timed replays use its choice.
@@ -435,7 +436,7 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
         trials = []
     else:
         knobs, default_ms, tuned_ms, trials = tune(
-            lambda: EventPeeler(*arrays, capacities=capacities), replays=5)
+            lambda: EventPeeler(*arrays, capacities=capacities, predicates=form), replays=5)
     p.set_tuning(**knobs)
     p.capture()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
@@ -489,7 +490,7 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
     if e2e_steps:
         from peel_b200.pipeline import PeelStream
 
-        stream_peeler = PeelStream(arrays, capacities, tuning=knobs)
+        stream_peeler = PeelStream(arrays, capacities, tuning=knobs, predicates=form)
         pipelined_steps = max(e2e_steps, 4 * e2e_steps)
         stream_peeler.submit(pinned)  # warm-up submission, collected untimed
         stream_peeler.finish()
@@ -595,18 +596,19 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
         # the filters' escalation rates.
         del p
         timed = {}
-        for form in ("binary64", "filtered", "filtered64"):
-            if form == DEFAULT_FORM:
+        for other_form in ("binary64", "filtered", "filtered64"):
+            if other_form == form:
                 continue
-            other, _ = fit_event_capacities(arrays, capacities, predicates=form)
+            other, _ = fit_event_capacities(arrays, capacities, predicates=other_form)
             other.set_tuning(**knobs)
             other.capture()
             for _ in range(args.warmup):
                 other.run()
             ms = time_replays(other, steps, flush)
             info = other.read_status()
-            timed[form] = {"ms": ms, "output": {k: info[k] for k in ("polygons", "triangles",
-                                                                     "layers")},
+            timed[other_form] = {"ms": ms, "output": {k: info[k] for k in ("polygons",
+                                                                           "triangles",
+                                                                           "layers")},
                            "stages_ms": stage_medians(other, 7, flush)}
             del other
         counted, _ = fit_event_capacities(arrays, capacities, predicates="counted")
@@ -614,8 +616,9 @@ def measure_config(config, args, rank, world, local_rank, steps, e2e_steps, cpu_
         counts = counted.predicate_counts()
         del counted
         result["predicates"] = {
-            "form": DEFAULT_FORM, "ms": ms_per_mesh, "others": timed,
-            "binary64_over_default": timed["binary64"]["ms"] / ms_per_mesh,
+            "form": form, "ms": ms_per_mesh, "others": timed,
+            "binary64_over_default": (timed["binary64"]["ms"] / ms_per_mesh
+                                      if "binary64" in timed else 1.0),
             "counts": counts,
             "escalated_share": {c: (v["binary64"] + v["exact"]) / max(1, sum(v.values()))
                                 for c, v in counts.items()},
@@ -691,6 +694,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="knot-65536")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--predicates", default=DEFAULT_FORM,
+                    choices=("filtered64", "filtered", "binary64"),
+                    help="predicate form of the timed extraction (the EventPeeler default: "
+                         "filtered64)")
     ap.add_argument("--quick", action="store_true",
                     help="skip the autotuner, the CPU baseline and the end-to-end leg "
                          "(for profiler runs)")
