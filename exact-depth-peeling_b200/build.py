@@ -5,7 +5,9 @@
 Every .cu file under csrc/ is compiled for compute_100a / sm_100a with
 binary64 contraction disabled (-fmad=false: predicates are plain IEEE and a
 CPU restatement of an expression gives the same bits) and linked into
-peel_b200/libedp_b200.so, next to the Python package that loads it.
+peel_b200/libedp_b200.so, next to the Python package that loads it.  The
+host-only exact intersection resolver (csrc/edp_resolve.cpp) is compiled
+with g++ into peel_b200/libedp_resolve.so.
 """
 
 import argparse
@@ -20,6 +22,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIBRARY = HERE / "peel_b200" / "libedp_b200.so"
+RESOLVER = HERE / "peel_b200" / "libedp_resolve.so"  # host C++ (exact resolver)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-I", str(HERE.parent / "include")]
@@ -60,6 +63,20 @@ def compile_one(src, extra):
     return obj
 
 
+def build_resolver(force=False):
+    """The exact intersection resolver: host C++ (g++), no CUDA."""
+    src = CSRC / "edp_resolve.cpp"
+    deps = [src, HERE.parent / "include/edp_resolve.h"]
+    if force or stale(RESOLVER, deps):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-std=c++17", "-O3", "-fPIC", "-shared", "-pthread", "-Wall",
+               "-I", str(HERE.parent / "include"), str(src), "-o", str(RESOLVER)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed on {src.name}:\n{r.stderr}")
+    return RESOLVER
+
+
 def build(force=False, verbose_ptxas=False):
     BUILD.mkdir(exist_ok=True)
     if force:
@@ -73,6 +90,7 @@ def build(force=False, verbose_ptxas=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_resolver(force)
     return LIBRARY
 
 

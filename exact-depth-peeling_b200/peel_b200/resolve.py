@@ -25,17 +25,28 @@ Construction (this module's own; the reference calls CGAL's autorefine):
    crossing then share its edges, which makes them non-manifold edges: the
    contours the resolved-mesh topology keeps (src/peel_common.h:100-123).
 4. A piece that stayed a triangle is written as is; any other piece is
-   written as a fan around its vertex average, in the parent's winding.
+   written as a fan, in the parent's winding: from its first corner (a
+   vertex not collinear with its neighbours) whose neighbours are corners
+   too, or else around the centroid of its first three corners.
+
+Two implementations of the same construction give identical output: the host
+C++ library libedp_resolve.so (include/edp_resolve.h: exact integer
+arithmetic on the scene's binary64 coordinates, all host threads), used
+whenever every input coordinate is a binary64 value and the library is built,
+and the arbitrary-precision rational code below, used otherwise (rational
+inputs, or numbers beyond the native size limit).
 
 Unlike the reference's importer, the input need not be a manifold: any
 triangle soup without coplanar overlaps is accepted.  Zero-area input
 triangles pass through unchanged.
 """
 
+import ctypes
 import json
 import sys
 import time
 from fractions import Fraction as Q
+from pathlib import Path
 
 import numpy as np
 
@@ -178,10 +189,7 @@ def coplanar_contact(fa, fb):
             return []
     area2 = sum(orient(poly[0][0], poly[i][0], poly[i + 1][0]) for i in range(1, len(poly) - 1))
     if area2 != 0:
-        raise ResolveError(
-            f"Triangles {fa.record.get('id', fa.index)} and {fb.record.get('id', fb.index)} "
-            "overlap on one plane with positive area; coincident surfaces are outside the "
-            "resolved-mesh contract")
+        raise overlap_error(fa, fb)
     return [p3 for _, p3 in poly]
 
 
@@ -299,12 +307,20 @@ def candidate_pairs(lo, hi):
     return pairs
 
 
-def resolve(data):
-    """The resolved scene (a new dict) and a summary of the preprocessing."""
+def resolve(data, native=None):
+    """The resolved scene (a new dict) and a summary of the preprocessing.
+
+    `native` None picks the C++ library when every coordinate is binary64
+    and the library is built; True requires it, False uses the rational
+    code."""
     start = time.perf_counter()
     triangles = data["triangles"]
     faces = [Face(i, t) for i, t in enumerate(triangles)]
     import_seconds = time.perf_counter() - start
+    if native is not False:
+        done = _resolve_native(data, faces, import_seconds, required=bool(native))
+        if done is not None:
+            return done
     start = time.perf_counter()
     live = [f for f in faces if not f.degenerate]
     if live:
@@ -365,6 +381,7 @@ def resolve(data):
     summary = {
         "method": "exact rational line splitting with shared-edge insertion",
         "arithmetic": "exact rational constructions",
+        "implementation": "python",
         "input_triangles": len(triangles),
         "output_triangles": len(out),
         "intersection_segments": segments,
@@ -377,6 +394,179 @@ def resolve(data):
     result["triangles"] = out
     if "original_triangles" not in result:
         result["original_triangles"] = triangles
+    result["intersection_preprocessing"] = summary
+    return result, summary
+
+
+# ---------------------------------------------------------------- native
+
+NATIVE = Path(__file__).resolve().parent / "libedp_resolve.so"
+_native_lib = None
+
+
+def native_library():
+    """ctypes handle of libedp_resolve.so, or None when it is not built."""
+    global _native_lib
+    if _native_lib is None and NATIVE.exists():
+        lib = ctypes.CDLL(str(NATIVE))
+        P, I64 = ctypes.c_void_p, ctypes.c_int64
+        lib.edp_resolve_abi_version.restype = ctypes.c_int
+        lib.edp_resolve.argtypes = [P, I64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+        lib.edp_resolve.restype = ctypes.c_int
+        lib.edp_resolution_triangles.argtypes = [P]
+        lib.edp_resolution_triangles.restype = I64
+        lib.edp_resolution_summary.argtypes = [P, P]
+        lib.edp_resolution_summary.restype = None
+        lib.edp_resolution_binary64.argtypes = [P, P, P]
+        lib.edp_resolution_binary64.restype = ctypes.c_int
+        lib.edp_resolution_exact.argtypes = [P, P, I64]
+        lib.edp_resolution_exact.restype = I64
+        lib.edp_resolution_overlap.argtypes = [P, P, P]
+        lib.edp_resolution_overlap.restype = None
+        lib.edp_resolution_free.argtypes = [P]
+        lib.edp_resolution_free.restype = None
+        if lib.edp_resolve_abi_version() != 1:
+            raise RuntimeError(f"{NATIVE.name}: unexpected ABI version")
+        _native_lib = lib
+    return _native_lib
+
+
+class NativeResolution:
+    """One run of the C++ resolver over binary64 triangles [T, 3, 3]."""
+
+    TOO_LARGE, BAD_INPUT = 2, 3
+
+    def __init__(self, triangles, threads=0, exact_text=False):
+        lib = native_library()
+        if lib is None:
+            raise RuntimeError(f"{NATIVE.name} is not built (exact-depth-peeling_b200/build.py)")
+        tri = np.ascontiguousarray(triangles, dtype=np.float64).reshape(-1, 9)
+        self._lib = lib
+        self._handle = ctypes.c_void_p()
+        self.status = lib.edp_resolve(tri.ctypes.data, tri.shape[0], int(threads),
+                                      int(bool(exact_text)), ctypes.byref(self._handle))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        if self._handle:
+            self._lib.edp_resolution_free(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def overlap(self):
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        self._lib.edp_resolution_overlap(self._handle, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def summary(self):
+        s = np.zeros(6, dtype=np.int64)
+        self._lib.edp_resolution_summary(self._handle, s.ctypes.data)
+        keys = ("intersection_segments", "cut_triangles", "candidate_pairs", "exact_pairs",
+                "points", "scale_exponent")
+        return dict(zip(keys, (int(v) for v in s)))
+
+    def arrays(self):
+        """(triangles [T, 3, 3] correctly rounded, parents [T] input indices)."""
+        t = int(self._lib.edp_resolution_triangles(self._handle))
+        vertices = np.empty((t, 3, 3), dtype=np.float64)
+        parents = np.empty(t, dtype=np.int64)
+        self._lib.edp_resolution_binary64(self._handle, vertices.ctypes.data, parents.ctypes.data)
+        return vertices, parents
+
+    def exact(self):
+        """Per output corner the exact coordinates as (X, Y, Z, W) integers;
+        the value is (X, Y, Z) / (W 2^E)."""
+        size = int(self._lib.edp_resolution_exact(self._handle, None, 0))
+        buf = ctypes.create_string_buffer(size)
+        self._lib.edp_resolution_exact(self._handle, buf, size)
+        return [tuple(int(h, 16) for h in line.split())
+                for line in buf.value.decode().split("\n") if line]
+
+
+def overlap_error(fa, fb):
+    return ResolveError(
+        f"Triangles {fa.record.get('id', fa.index)} and {fb.record.get('id', fb.index)} "
+        "overlap on one plane with positive area; coincident surfaces are outside the "
+        "resolved-mesh contract")
+
+
+def resolve_arrays(triangles, threads=0):
+    """Resolve a binary64 triangle soup [T, 3, 3] with the C++ resolver:
+    returns (triangles [T', 3, 3], the exact pieces correctly rounded to
+    binary64; parents [T'], each piece's input triangle; summary)."""
+    with NativeResolution(triangles, threads) as r:
+        if r.status == 1:
+            a, b = r.overlap()
+            raise ResolveError(f"Triangles {a} and {b} overlap on one plane with positive area; "
+                               "coincident surfaces are outside the resolved-mesh contract")
+        if r.status:
+            raise RuntimeError(f"native resolver failed with status {r.status}")
+        vertices, parents = r.arrays()
+        return vertices, parents, r.summary()
+
+
+def _binary64(q):
+    try:
+        x = float(q)
+    except OverflowError:
+        return None
+    return x if Q(x) == q else None
+
+
+def _resolve_native(data, faces, import_seconds, required):
+    """resolve() through the C++ library; None when it does not apply (not
+    built, rational inputs, numbers beyond its limits) and not `required`."""
+    if native_library() is None:
+        if required:
+            raise RuntimeError(f"{NATIVE.name} is not built (exact-depth-peeling_b200/build.py)")
+        return None
+    coords = [_binary64(c) for f in faces for p in f.v for c in p]
+    if any(c is None for c in coords):
+        if required:
+            raise ValueError("the native resolver takes binary64 coordinates only")
+        return None
+    start = time.perf_counter()
+    tri = np.array(coords, dtype=np.float64).reshape(-1, 3, 3)
+    with NativeResolution(tri, exact_text=True) as r:
+        if r.status == 1:
+            a, b = r.overlap()
+            raise overlap_error(faces[a], faces[b])
+        if r.status in (NativeResolution.TOO_LARGE, NativeResolution.BAD_INPUT) and not required:
+            return None
+        if r.status:
+            raise RuntimeError(f"native resolver failed with status {r.status}")
+        info = r.summary()
+        _, parents = r.arrays()
+        corners = r.exact()
+    scale = info["scale_exponent"]
+    out = []
+    for t, parent in enumerate(parents):
+        record = faces[int(parent)].record
+        source = record.get("original_source_id", record.get("id", int(parent)))
+        mesh_face = record.get("mesh_face_id", source)
+        vertices = []
+        for x, y, z, w in corners[3 * t:3 * t + 3]:
+            den = w << scale
+            vertices.append([text(Q(x, den)), text(Q(y, den)), text(Q(z, den))])
+        out.append({"id": len(out), "original_source_id": source, "mesh_face_id": mesh_face,
+                    "vertices": vertices})
+    summary = {
+        "method": "exact rational line splitting with shared-edge insertion",
+        "arithmetic": "exact rational constructions",
+        "implementation": "native",
+        "input_triangles": len(faces),
+        "output_triangles": len(out),
+        "intersection_segments": info["intersection_segments"],
+        "cut_triangles": info["cut_triangles"],
+        "import_seconds": import_seconds,
+        "refinement_seconds": time.perf_counter() - start,
+        "positive_area_coincident_surfaces_supported": False,
+    }
+    result = dict(data)
+    result["triangles"] = out
+    if "original_triangles" not in result:
+        result["original_triangles"] = data["triangles"]
     result["intersection_preprocessing"] = summary
     return result, summary
 
@@ -415,12 +605,21 @@ def insert_points(poly, points, cloud):
 
 
 def fan(poly):
-    """Triangles of a convex piece: itself when it is one, else a fan around
-    its vertex average (every boundary edge kept, no T-junctions)."""
+    """Triangles of a convex piece: itself when it is one; else a fan from its
+    first corner whose two neighbours are corners too (no point inserted on
+    the edges at that corner, so no fan triangle is degenerate), or, when
+    every corner has an inserted neighbour, a fan around the centroid of its
+    first three corners.  Corners are vertices not collinear with their
+    neighbours; every boundary edge is kept, so there are no T-junctions."""
     if len(poly) == 3:
         return [poly]
     n = len(poly)
-    center = tuple(sum(p[c] for p in poly) / n for c in range(3))
+    corner = [not collinear(poly[i - 1], poly[(i + 1) % n], poly[i]) for i in range(n)]
+    for v in range(n):
+        if corner[v] and corner[v - 1] and corner[(v + 1) % n]:
+            return [[poly[v], poly[(v + t) % n], poly[(v + t + 1) % n]] for t in range(1, n - 1)]
+    corners = [poly[i] for i in range(n) if corner[i]]
+    center = tuple(sum(p[c] for p in corners[:3]) / 3 for c in range(3))
     return [[center, poly[i], poly[(i + 1) % n]] for i in range(n)]
 
 

@@ -235,6 +235,13 @@ def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7, directio
             else:
                 break
         side *= 1.1
+    vertices, faces = _primitives(radii, kinds, budget, centers, noise, rng)
+    return vertices, faces, *_primitive_camera(vertices, direction)
+
+
+def _primitives(radii, kinds, budget, centers, noise, rng):
+    """One mesh of noisy spheres (kind 0) and tori (kind 1) of the given
+    bounding radii, face budgets and centres."""
     parts_v, parts_f, offset = [], [], 0
     for r, kind, faces, c in zip(radii, kinds, budget, centers):
         if kind == 0:
@@ -248,14 +255,74 @@ def packed_primitives(total_faces=720000, count=40, noise=0.02, seed=7, directio
         parts_v.append(v + c)
         parts_f.append(f + offset)
         offset += len(v)
-    vertices = np.concatenate(parts_v)
-    faces = np.concatenate(parts_f).astype(np.int32)
+    return np.concatenate(parts_v), np.concatenate(parts_f).astype(np.int32)
+
+
+def _primitive_camera(vertices, direction):
+    """The 60 degree pinhole at 3x the bounding radius from `direction`
+    (default (0.3, 0.4, 3))."""
     centroid = vertices.mean(0)
     bound = np.linalg.norm(vertices - centroid, axis=1).max()
     view = np.array([0.3, 0.4, 3.0]) if direction is None else np.asarray(direction, float)
     camera, settings = _pinhole(centroid + view / np.linalg.norm(view) * 3 * bound, centroid,
                                 near=0.01 * bound)
-    return vertices, faces, camera, settings
+    return camera, settings
+
+
+def overlapping_primitives(total_faces=720000, count=40, noise=0.02, seed=7, direction=None):
+    """``count`` noisy spheres and tori (bounding radii log-uniform in
+    [0.05, 0.5], faces in proportion to surface area, about ``total_faces`` in
+    all) with centres uniform in the unit box, free to overlap: an
+    unresolved triangle soup (vertices, faces, camera, settings) whose
+    surfaces cross."""
+    rng = np.random.default_rng(seed)
+    radii = np.exp(rng.uniform(np.log(0.05), np.log(0.5), size=count))
+    kinds = rng.integers(0, 2, size=count)  # 0 sphere, 1 torus
+    area = np.where(kinds == 0, 4 * np.pi * radii ** 2, 4 * np.pi ** 2 * (0.7 * radii) * (0.3 * radii))
+    budget = total_faces * area / area.sum()
+    centers = rng.uniform(0.0, 1.0, size=(count, 3))
+    vertices, faces = _primitives(radii, kinds, budget, centers, noise, rng)
+    return vertices, faces, *_primitive_camera(vertices, direction)
+
+
+def resolve_mesh(vertices, faces, threads=0):
+    """The resolved mesh of a triangle soup: every crossing split exactly by
+    the C++ resolver (peel_b200.resolve), pieces rounded to binary64 and
+    their equal corners welded.  Returns (vertices, faces, parents: each
+    face's input face, summary)."""
+    from .resolve import resolve_arrays
+
+    tris, parents, summary = resolve_arrays(vertices[faces], threads)
+    corners = tris.reshape(-1, 3)
+    unique, index = np.unique(corners, axis=0, return_inverse=True)
+    return unique, index.reshape(-1, 3).astype(np.int32), parents, summary
+
+
+def resolved_primitives(total_faces=720000, count=40, noise=0.02, seed=7, direction=None):
+    """The overlapping primitives (overlapping_primitives) resolved
+    (resolve_mesh): about 720K input faces by default; every face of the
+    result lies on one input face (resolution_info gives the map).  The
+    camera is the packed primitives' one.  Returns (vertices, faces, camera,
+    settings)."""
+    key = (total_faces, count, noise, seed)
+    if key not in _RESOLVED:
+        v, f, camera, settings = overlapping_primitives(total_faces, count, noise, seed)
+        rv, rf, parents, summary = resolve_mesh(v, f)
+        _RESOLVED[key] = (rv, rf, camera, settings, parents, summary, v, f)
+    rv, rf, camera, settings = _RESOLVED[key][:4]
+    if direction is not None:
+        camera, settings = _primitive_camera(_RESOLVED[key][6], direction)
+    return rv, rf, camera, settings
+
+
+_RESOLVED = {}  # resolved_primitives() results by arguments (the resolution takes seconds)
+
+
+def resolution_info(total_faces=720000, count=40, noise=0.02, seed=7):
+    """(parents, resolver summary, input vertices, input faces) of a
+    resolved_primitives() call made before."""
+    entry = _RESOLVED[(total_faces, count, noise, seed)]
+    return entry[4], entry[5], entry[6], entry[7]
 
 
 def training_mesh(seed):
@@ -393,6 +460,7 @@ def _random_rotation(rng):
 
 
 CONFIGS = {
+    "overlap-720k": resolved_primitives,
     "primitives-720k": packed_primitives,
     "icospheres-2560": nested_icospheres,
     "knot-65536": knot_tube,
