@@ -217,6 +217,25 @@ def test_primitives_720k_sampled_ranks_and_conservation():
     check_vertex_error(p, samples=1000)
 
 
+def test_overlap_720k_sampled_ranks_and_conservation():
+    """Config 5 as named: the 40 primitives placed with overlap (720,916
+    faces) and resolved exactly on the host (1,218,926 faces, every crossing a
+    shared edge): 3,000 exact ranks drawn per layer, exact vertex error,
+    conservation of every source and the mesh checksum."""
+    from peel_b200 import scenes
+
+    host = scenes.resolved_primitives()
+    assert scenes.resolution_info()[1]["intersection_segments"] > 10000
+    p = run("events", host)
+    polys = parity.polygons(p)
+    info = p.read_status()
+    assert info["layers"] >= 10
+    check_conservation(p, host, polys)
+    check_mesh_checksum(p, polys)
+    assert check_sampled_ranks(host, polys, samples=3000) >= 2940
+    check_vertex_error(p, samples=1000)
+
+
 def test_batched_128_every_scene_sampled():
     """Config 4: one graph replay of all 128 scenes (64 turntable views of the
     genus-3 surface, 64 packed-primitive meshes); in every scene 160 exact
