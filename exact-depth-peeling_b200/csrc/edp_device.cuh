@@ -41,7 +41,10 @@ enum Metric : int {
   kRounds, kUniqueContours, kHeavyRayGroups, kBeamAttempts, kCertifiedBeams,
   kBeamCandidateTests, kHeavyBeams, kRankComponents, kRankConnections,
   kConnectionContourTests, kMergedPolygons, kMatchedPatchEdges, kEdgeHashMisses,
-  kHeavyNodedPolygons, kMetrics
+  kHeavyNodedPolygons,
+  // Filtered binary64 predicates: work the filter-only kernels left to the
+  // exact passes (parked patches, containment tests, hit groups, polygons).
+  kParkedPatches, kDeferredContainTests, kDeferredHitGroups, kDeferredPolygons, kMetrics
 };
 
 // ---------------------------------------------------------------- vectors

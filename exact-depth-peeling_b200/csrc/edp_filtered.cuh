@@ -10,7 +10,10 @@
 //      class and deciding stage into Dev::pred_counts;
 //   3  filtered from binary64: the same exact signs with the binary32 stage
 //      skipped (orientation through orient2d_lean, the binary64 filter as one
-//      bound test, then expansion arithmetic).
+//      bound test, then expansion arithmetic);
+//   4  the binary64 filters of form 3 alone, for kernels whose undecided
+//      cases go to a second pass in form 3 (pred::kUndecided marks them).
+//      Where form 4 decides, it gives form 3's sign.
 // Constructions (intersection points, clip parameters, depths stored for the
 // hit sort's radix fallback) stay binary64 in every form.
 #pragma once
@@ -71,6 +74,8 @@ __device__ inline int side_sign(V2 a, V2 b, V2 c, int &stage) {
     return sign_of(cross(a, b, c));
   } else if constexpr (F == 3) {
     return pred::orient2d_lean(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
+  } else if constexpr (F == 4) {
+    return pred::orient2d_filter(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
   } else {
     return pred::orient2d(a.x, a.y, b.x, b.y, c.x, c.y, &stage);
   }
@@ -92,7 +97,10 @@ __device__ inline int order_sign(const Plane &s1, double z1, const Plane &s2, do
     }
     const double p[6] = {s1.a, s1.b, s1.c, s2.a, s2.b, s2.c};
     const double q[6] = {x.x, x.y, 1.0, -x.x, -x.y, -1.0};
-    return pred::dot_sign(p, q, 6, &stage, F != 3);
+    if constexpr (F == 4)
+      return pred::dot_sign_filter(p, q, 6, &stage);
+    else
+      return pred::dot_sign(p, q, 6, &stage, F != 3);
   }
 }
 

@@ -72,7 +72,16 @@ struct Segments {
   const int2 *near_src;  // the sources whose planes give `near`
   const V2 *near_mag;    // their |a x| + |b y| + |c| at the ends
   const Plane *scores;
+  const int2 *vid;       // the welded mesh vertex at each end, or -1
+  const int *faces, *canonical, *clipped, *src_n;
 };
+
+// Source `s` is an unclipped triangle with welded vertex `v`.
+__device__ inline bool has_vertex(const Segments &g, int s, int v) {
+  if (v < 0 || g.clipped[s] || g.src_n[s] != 3) return false;
+  const int *f = g.faces + 3 * int64_t(s);
+  return g.canonical[f[0]] == v || g.canonical[f[1]] == v || g.canonical[f[2]] == v;
+}
 
 // Predicate tallies of one subdivision warp (counted form only).
 struct CutTally {
@@ -84,15 +93,20 @@ struct CutTally {
 // form (edp_filtered.cuh): the plain form evaluates the reference's binary64
 // expressions; the filtered forms take exact signs of the sides, of the
 // segment ends against the patch edges and of the depth differences, and
-// keep binary64 for the clip parameters.
+// keep binary64 for the clip parameters.  The filter-only form returns
+// kDeferAt - k when its filters cannot decide candidate k (no candidate
+// before k cuts): the patch is then finished by the exact pass from k on.
+constexpr int kDeferAt = -2;
+
 template <int F>
 __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 q, int n,
-                                const Plane &sc, V2 &a, V2 &b, int &side, CutTally &tally) {
+                                const Plane &sc, int source, V2 &a, V2 &b, int &side,
+                                CutTally &tally) {
   const int lane = threadIdx.x & 31;
   const bool mine = lane < n;
   const int width = lane_width(n);
   V2 ca = v2(0.0, 0.0), cb = ca, cn = ca, cm = ca;
-  int2 cs = make_int2(0, 0);
+  int2 cs = make_int2(0, 0), cv = make_int2(-1, -1);
   if ((batch >> lane) & 1u) {
     const int c = __ldg(&g.ids[first + lane]);
     ca = g.a[c];
@@ -101,6 +115,7 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
     if constexpr (F != 0) {
       cs = g.near_src[c];
       cm = g.near_mag[c];
+      cv = g.vid[c];
     }
   }
   while (batch) {
@@ -115,6 +130,8 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
       side = mine ? side_sign<F>(a, b, p, stage) : 0;
       if constexpr (F == 2)
         if (mine) tally.side.add(stage);
+      if constexpr (F == 4)
+        if (__any_sync(kFull, side == pred::kUndecided)) return kDeferAt - k;
     }
     if (!__ballot_sync(kFull, mine && side > 0) || !__ballot_sync(kFull, mine && side < 0))
       continue;
@@ -128,27 +145,36 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
       // The patch's depth plane against the plane of the source that gives
       // the segment its near depth, at the segment's ends.  Each binary64
       // evaluation is within 3.01 u of its terms' magnitudes (two products,
-      // two sums), so a difference above 4 u of both magnitudes has its sign;
-      // otherwise the two planes are compared exactly (zero when the
-      // source is the patch's own).
+      // two sums), so a difference above 4 u of both magnitudes has its sign.
+      // Otherwise: zero when the end is a mesh vertex of both triangles (both
+      // planes pass through it: the projected mesh's exact depths tie there,
+      // which the rounded plane coefficients can only approximate), else the
+      // two planes compared exactly (zero when the source is the patch's
+      // own).
       int stage_b = 0;
       const V2 mag = shfl(cm, k);
       const double bound_a = 4.0 * pred::kU64 *
           (fabs(sc.a * a.x) + fabs(sc.b * a.y) + fabs(sc.c) + mag.x);
       const double bound_b = 4.0 * pred::kU64 *
           (fabs(sc.a * b.x) + fabs(sc.b * b.y) + fabs(sc.c) + mag.y);
+      const int sa = __shfl_sync(kFull, cs.x, k), sb = __shfl_sync(kFull, cs.y, k);
+      const int va = __shfl_sync(kFull, cv.x, k), vb = __shfl_sync(kFull, cv.y, k);
       if (fabs(za) > bound_a) {
         sza = sign_of(za);
         stage = pred::kBinary64;
+      } else if (has_vertex(g, source, va) && has_vertex(g, sa, va)) {
+        sza = 0;
+        stage = pred::kBinary64;
       } else {
-        const int sa = __shfl_sync(kFull, cs.x, k);
         sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
       }
       if (fabs(zb) > bound_b) {
         szb = sign_of(zb);
         stage_b = pred::kBinary64;
+      } else if (has_vertex(g, source, vb) && has_vertex(g, sb, vb)) {
+        szb = 0;
+        stage_b = pred::kBinary64;
       } else {
-        const int sb = __shfl_sync(kFull, cs.y, k);
         szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
       }
       if constexpr (F == 2) {
@@ -157,6 +183,8 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
           tally.depth.add(stage_b);
         }
       }
+      if constexpr (F == 4)
+        if (sza == pred::kUndecided || szb == pred::kUndecided) return kDeferAt - k;
     }
     if (sza <= 0 && szb <= 0) continue;
     const double da = cross(p, q, a), db = cross(p, q, b);
@@ -174,6 +202,9 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
           tally.segment.add(stage_b);
         }
       }
+      if constexpr (F == 4)
+        if (__any_sync(kFull, sda == pred::kUndecided || sdb == pred::kUndecided))
+          return kDeferAt - k;
     }
     if (__ballot_sync(kFull, mine && sda <= 0 && sdb <= 0)) continue;
     double low, high, rz;
@@ -320,6 +351,29 @@ __device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int
   return true;
 }
 
+// Park a patch at the top of the next frontier `f` for this round's exact
+// pass (from its cursor on); false when the frontier is full.  `parked`
+// counts the parked patches.
+__device__ __noinline__ bool defer_patch(Frontier f, int *parked, V2 p, int n, int source,
+                                         int cursor) {
+  const int lane = threadIdx.x & 31;
+  int k = 0;
+  if (lane == 0) k = atomicAdd(parked, 1);
+  k = __shfl_sync(kFull, k, 0);
+  const int64_t slot = f.capacity - 1 - k;
+  if (slot < 0) {
+    if (lane == 0) set_error(f.status, kErrResidual);
+    return false;
+  }
+  if (lane < n) f.v[int64_t(kMaxVertices) * slot + lane] = p;
+  if (lane == 0) {
+    f.n[slot] = n;
+    f.src[slot] = source;
+    f.cur[slot] = cursor;
+  }
+  return true;
+}
+
 // One frontier round, one patch per warp (frontier.py:106-223).  A patch
 // meets the contour segments whose boxes overlap its own in leaf order,
 // starting at its cursor (the first leaf it has not met).  The first segment
@@ -331,31 +385,45 @@ __device__ __noinline__ bool push_patch(Frontier f, V2 p, int n, int source, int
 // tested against the part's box when they are expanded.  A patch that has
 // met every candidate is final and goes to the output pool; one that spends
 // its budget carries over.  Warps take patches from a shared counter.
+//
+// With filtered binary64 predicates the round runs twice: the filter-only
+// form (F = 4, no exact stage, so fewer registers and less code) over the
+// frontier, parking every patch whose filters cannot decide a test at the top
+// of the next frontier with its cursor at that test; then form 3, with the
+// exact stages, over the parked patches (`deferred_pass`).  Each patch meets
+// the same tests in the same order as in one form-3 pass, so the output is
+// the same.
 template <int F>
-__global__ void __launch_bounds__(kBlock, F == 0 ? 5 : 4) k_subdivide(Dev d) {
+__global__ void __launch_bounds__(kBlock, (F == 0 || F == 4) ? 5 : 4)
+    k_subdivide(Dev d, int deferred_pass) {
   __shared__ V2 s_parts[kWarps][2][kMaxVertices];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   V2 *left_part = s_parts[warp][0], *right_part = s_parts[warp][1];
   const int par = *d.parity;
-  const V2 *fv = d.fv[par];
-  const int *fn = d.fn[par], *fsrc = d.fsrc[par], *fcur = d.fcur[par];
-  const int live = int(min(int64_t(d.status[kResidual]), d.cap.frontier));
+  const int from = deferred_pass ? par ^ 1 : par;
+  const V2 *fv = d.fv[from];
+  const int *fn = d.fn[from], *fsrc = d.fsrc[from], *fcur = d.fcur[from];
+  const int parked = deferred_pass ? int(min(int64_t(d.sc[kDeferred]), d.cap.frontier)) : 0;
+  const int live = deferred_pass ? parked : int(min(int64_t(d.status[kResidual]), d.cap.frontier));
+  int *taken = deferred_pass ? &d.sc[kDeferredNext] : &d.sc[kFrontierNext];
   const int leaves = *d.seg_tree.size;
   const int next_lane = lane + 1;
   const Segments segs{d.seg_tree.ids, d.seg_a, d.seg_b, d.seg_near, d.seg_near_src,
-                      d.seg_near_mag, d.scores};
+                      d.seg_near_mag, d.scores, d.seg_vid, d.faces, d.canonical, d.clipped,
+                      d.src_n};
   const Frontier next{d.fv[par ^ 1], d.fn[par ^ 1], d.fsrc[par ^ 1], d.fcur[par ^ 1],
-                      &d.status[kNextResidual], d.status, d.cap.frontier};
+                      &d.status[kNextResidual], d.status, d.cap.frontier - parked};
   long long visits = 0, tests = 0, splits = 0;  // lane 0's tallies
   CutTally tally;
   for (;;) {
     int i = 0, failed = 0;
     if (lane == 0) {
-      i = atomicAdd(&d.sc[kFrontierNext], 1);
+      i = atomicAdd(taken, 1);
       failed = *(volatile int *)&d.status[kError];
     }
     i = __shfl_sync(kFull, i, 0);
     if (i >= live || __shfl_sync(kFull, failed, 0) != 0) break;
+    if (deferred_pass) i = int(d.cap.frontier) - 1 - i;  // parked from the top down
     int n = fn[i];
     if (n == 0) continue;
     ++visits;
@@ -376,12 +444,24 @@ __global__ void __launch_bounds__(kBlock, F == 0 ? 5 : 4) k_subdivide(Dev d) {
     walk_begin(w, d.seg_tree, leaves, lo, hi, cursor);
     for (;;) {
       unsigned batch;
-      int first, resume = leaves, cut = -1, side = 0;
+      int first, resume = leaves, cut = -1, side = 0, defer = -1;
       V2 a, b;
       while (walk_next(w, d.seg_tree, leaves, lo, hi, cursor, budget, batch, first, resume)) {
-        cut = first_cut<F>(segs, batch, first, p, q, n, sc, a, b, side, tally);
+        cut = first_cut<F>(segs, batch, first, p, q, n, sc, source, a, b, side, tally);
+        if constexpr (F == 4) {
+          if (cut <= kDeferAt) {
+            defer = first + (kDeferAt - cut);
+            break;
+          }
+        }
         tests += __popc(cut >= 0 ? batch & (kFull >> (31 - cut)) : batch);  // met up to the cut
         if (cut >= 0) break;
+      }
+      if constexpr (F == 4) {
+        if (defer >= 0) {
+          defer_patch(next, &d.sc[kDeferred], p, n, source, defer);
+          break;
+        }
       }
       if (cut < 0) {
         if (resume < leaves) {
@@ -440,8 +520,14 @@ __global__ void __launch_bounds__(kBlock, F == 0 ? 5 : 4) k_subdivide(Dev d) {
 }
 
 // Swap frontiers and decide whether another round runs (event_kernels.py:12-25).
+// Patches parked for the exact pass shared the next frontier's slots from the
+// top: together with the pushed ones they must have fit.
 __global__ void k_advance(Dev d) {
   int next = d.status[kNextResidual];
+  if (int64_t(next) + d.sc[kDeferred] > d.cap.frontier) set_error(d.status, kErrResidual);
+  d.metrics[kParkedPatches] += d.sc[kDeferred];
+  d.sc[kDeferred] = 0;
+  d.sc[kDeferredNext] = 0;
   d.status[kResidual] = next;
   d.status[kNextResidual] = 0;
   d.sc[kFrontierNext] = 0;
@@ -459,7 +545,13 @@ __global__ void k_advance(Dev d) {
 cudaError_t stage_step(const Dev &d, cudaStream_t st) {
   int64_t g = ceil_div(d.cap.frontier, kWarps);
   if (g > 148 * int64_t(d.subdivide_blocks)) g = 148 * int64_t(d.subdivide_blocks);
-  EDP_LAUNCH_FORM(d.predicates, k_subdivide, unsigned(g), kBlock, st, d);
+  if (d.predicates == 3) {  // filtered binary64: filter-only pass, then the exact pass
+    k_subdivide<4><<<unsigned(g), kBlock, 0, st>>>(d, 0);
+    note_launch();
+    k_subdivide<3><<<unsigned(g), kBlock, 0, st>>>(d, 1);
+  } else {
+    EDP_LAUNCH_FORM(d.predicates, k_subdivide, unsigned(g), kBlock, st, d, 0);
+  }
   note_launch();
   k_advance<<<1, 1, 0, st>>>(d);
   note_launch();

@@ -124,7 +124,17 @@ enum Scalar : int {
   kClipHidden = 23,
   kClipParity = 24,
   kClipCondition = 25,
-  kScalarCount = 28
+  // Subdivision in the filter-only form: patches deferred to the exact pass
+  // this round (kept at the top of the next frontier), and the next of them
+  // an exact-pass warp takes.
+  kDeferred = 26,
+  kDeferredNext = 27,
+  // Ranks in the filter-only form: containment tests, hit groups and polygon
+  // searches left for the exact passes.
+  kRayDeferred = 28,
+  kSortDeferred = 29,
+  kAssignDeferred = 30,
+  kScalarCount = 32  // k_reset clears them with one warp
 };
 
 // Predicate tallies: six classes by three deciding stages (edp_filtered.cuh).
@@ -180,6 +190,7 @@ struct Dev {
   V2 *seg_a, *seg_b, *seg_near;
   int2 *seg_near_src;  // the sources whose depth planes give seg_near (exact depth tests)
   V2 *seg_near_mag;    // per end, |a x| + |b y| + |c| of that plane: the depth's error scale
+  int2 *seg_vid;       // per end, its welded mesh vertex (-1 when not a mesh vertex)
   float4 *seg_lo, *seg_hi;
   int *seg_table, *seg_min, *seg_slot;
   int seg_mask;
@@ -210,6 +221,12 @@ struct Dev {
   unsigned long long *hkeys, *hkeys_tmp;
   int *group_counts, *group_offsets;
   int *group_fill;  // hits placed in each group so far
+  // Filtered binary64 ranks: the (ray, source) containment tests, and then
+  // the hit groups and the polygons, whose binary64 filters left a sign
+  // undecided, for the exact passes.
+  int2 *ray_defer;
+  int64_t ray_defer_cap;
+  int *rank_defer;  // [regions]
   // Optional convex merging: each polygon's chosen patch edge, and the
   // compaction copy of the outputs (allocated with merge_regions only).
   int *merge_choice;

@@ -161,8 +161,13 @@ EDP_HD inline int orient2d(double ax, double ay, double bx, double by, double cx
 // Shewchuk's first binary64 filter as one bound test, then the exact stage.
 // Same sign as orient2d (inputs whose products underflow excepted, as for
 // Shewchuk's filter).
-EDP_HD inline int orient2d_lean(double ax, double ay, double bx, double by, double cx,
-                                double cy, int *stage = nullptr) {
+// Result of a filter-only predicate that its filter cannot decide: the
+// caller defers the whole decision to a pass with the exact stage.
+constexpr int kUndecided = 2;
+
+// orient2d_lean's binary64 filter alone: the sign, or kUndecided.
+EDP_HD inline int orient2d_filter(double ax, double ay, double bx, double by, double cx,
+                                  double cy, int *stage = nullptr) {
   const double detleft = (ax - cx) * (by - cy);
   const double detright = (ay - cy) * (bx - cx);
   const double det = detleft - detright;
@@ -172,7 +177,13 @@ EDP_HD inline int orient2d_lean(double ax, double ay, double bx, double by, doub
     return sign_of(det);
   }
   if (stage) *stage = kExact;
-  return orient2d_exact(ax, ay, bx, by, cx, cy);
+  return kUndecided;
+}
+
+EDP_HD inline int orient2d_lean(double ax, double ay, double bx, double by, double cx,
+                                double cy, int *stage = nullptr) {
+  const int s = orient2d_filter(ax, ay, bx, by, cx, cy, stage);
+  return s != kUndecided ? s : orient2d_exact(ax, ay, bx, by, cx, cy);
 }
 
 // ---------------------------------------------------------------- linear forms
@@ -191,6 +202,25 @@ EDP_HD inline EDP_COLD int dot_sign_exact(const double *p, const double *q, int 
     ++m;
   }
   return expansion_sign(e, m);
+}
+
+// dot_sign's binary64 stage alone: the bound of its binary32 stage with
+// binary64's unit roundoff, (n + 2) u S, taken with a margin as
+// 2 (n + 2) u s64.  The sign, or kUndecided.
+EDP_HD inline int dot_sign_filter(const double *p, const double *q, int n, int *stage = nullptr) {
+  double s64 = 0.0, a64 = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double t = p[k] * q[k];
+    s64 += t;
+    a64 += fabs(t);
+  }
+  const double bound64 = a64 * (2.0 * double(n + 2) * kU64);
+  if (s64 > bound64 || -s64 > bound64) {
+    if (stage) *stage = kBinary64;
+    return sign_of(s64);
+  }
+  if (stage) *stage = kExact;
+  return kUndecided;
 }
 
 // Sign of sum_k p[k] q[k] for n <= 8 terms (a plane evaluated at a point, or
@@ -222,21 +252,8 @@ EDP_HD inline int dot_sign(const double *p, const double *q, int n, int *stage =
       return s32 > 0.0f ? 1 : -1;
     }
   }
-  // Binary64 stage: the same bound with binary64's unit roundoff,
-  // (n + 2) u S, taken with a margin as 2 (n + 2) u s64.
-  double s64 = 0.0, a64 = 0.0;
-  for (int k = 0; k < n; ++k) {
-    const double t = p[k] * q[k];
-    s64 += t;
-    a64 += fabs(t);
-  }
-  const double bound64 = a64 * (2.0 * double(n + 2) * kU64);
-  if (s64 > bound64 || -s64 > bound64) {
-    if (stage) *stage = kBinary64;
-    return sign_of(s64);
-  }
-  if (stage) *stage = kExact;
-  return dot_sign_exact(p, q, n);
+  const int s = dot_sign_filter(p, q, n, stage);
+  return s != kUndecided ? s : dot_sign_exact(p, q, n);
 }
 
 }  // namespace pred

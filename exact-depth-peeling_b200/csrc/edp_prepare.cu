@@ -367,6 +367,19 @@ __global__ void k_segment_compact(Dev d) {
     const Plane pa = d.scores[near_src.x], pb = d.scores[near_src.y];
     d.seg_near_mag[c] = v2(fabs(pa.a * a.x) + fabs(pa.b * a.y) + fabs(pa.c),
                            fabs(pb.a * b.x) + fabs(pb.b * b.y) + fabs(pb.c));
+    // The welded mesh vertex at each end: the representative's polygon is its
+    // triangle's projection (unclipped; reversed when back-facing), so its
+    // vertex j is the face's vertex j, or 2 - j.
+    int2 vid = make_int2(-1, -1);
+    if (!d.clipped[own] && d.src_n[own] == 3) {
+      const V2 *p = d.src_v + int64_t(kSourceVertices) * own;
+      for (int j = 0; j < 3; ++j) {
+        const int v = d.canonical[d.faces[3 * int64_t(own) + (d.facing[own] < 0 ? 2 - j : j)]];
+        if (p[j] == a) vid.x = v;
+        if (p[j] == b) vid.y = v;
+      }
+    }
+    d.seg_vid[c] = vid;
     d.seg_lo[c] = make_float4(float(fmin(a.x, b.x) - 2.0e-7), float(fmin(a.y, b.y) - 2.0e-7),
                               float(fmin(za, zb) - pz), 0.f);
     d.seg_hi[c] = make_float4(float(fmax(a.x, b.x) + 2.0e-7), float(fmax(a.y, b.y) + 2.0e-7),
@@ -392,6 +405,8 @@ __global__ void k_seed(Dev d) {
     d.status[kResidual] = fits ? d.n : 0;
     d.status[kPeakResidual] = d.status[kResidual];
     d.sc[kFrontierNext] = 0;
+    d.sc[kDeferred] = 0;
+    d.sc[kDeferredNext] = 0;
   }
 }
 

@@ -499,6 +499,43 @@ __device__ inline bool contains_flat(const Dev &d, int source, V2 x, Tally &t) {
   return n > 0;
 }
 
+// contains_flat's answer (0 or 1) in forms 0-3; in the filter-only form 4,
+// pred::kUndecided when no edge's filtered sign excludes x and some edge's
+// filter left its sign undecided (the exact pass then decides: the answer is
+// the AND over the edges, so the order of the tests does not matter).
+template <int F>
+__device__ inline int contains_form(const Dev &d, int source, V2 x, Tally &t) {
+  if constexpr (F != 4) {
+    return contains_flat<F>(d, source, x, t) ? 1 : 0;
+  } else {
+    const V2 *p = d.src_v + int64_t(kSourceVertices) * source;
+    const int n = d.src_n[source];
+    bool undecided = false;
+    for (int j = 0; j < n; ++j) {
+      V2 a = p[j], b = p[(j + 1) % n];
+      int stage = 0;
+      const int s = side_sign<F>(a, b, x, stage);
+      if (s == pred::kUndecided) {
+        undecided = true;
+        continue;
+      }
+      bool owned = b.y > a.y || (b.y == a.y && b.x < a.x);
+      if (s < 0 || (s == 0 && !owned)) return 0;
+    }
+    return undecided ? pred::kUndecided : (n > 0 ? 1 : 0);
+  }
+}
+
+// Leave a containment test of ray group `group` against `source` to the exact
+// pass (k_ray_exact); the pool's overflow is a hit-pool overflow.
+__device__ inline void defer_contains(const Dev &d, int group, int source) {
+  const int k = atomicAdd(&d.sc[kRayDeferred], 1);
+  if (k < d.ray_defer_cap)
+    d.ray_defer[k] = make_int2(group, source);
+  else
+    set_error(d.status, kErrHits);
+}
+
 // ---------------------------------------------------------------- source grid
 // Grid column (or row) of a window coordinate: floor(v G) clamped to the grid.
 __device__ inline int ray_cell(double v, int g) {
@@ -611,7 +648,10 @@ __global__ void k_ray_hits(Dev d) {
         if (!overlaps(d.src_lo[s], d.src_hi[s], lo, hi)) continue;
         ++met;
         last = max(last, d.leaf_of[s]);
-        if (contains_flat<F>(d, s, x, contain)) {
+        const int inside = contains_form<F>(d, s, x, contain);
+        if (F == 4 && inside == pred::kUndecided) {
+          defer_contains(d, i, s);
+        } else if (inside) {
           hits.source[hits.count] = s;
           hits.depth[hits.count] = value(d.scores[s], x);
           ++found;
@@ -631,7 +671,10 @@ __global__ void k_ray_hits(Dev d) {
       node = query_next(d.source_tree, leaves, lo, hi, node, 0, s);
       if (s < 0) break;
       ++tests;
-      if (contains_flat<F>(d, s, x, contain)) {
+      const int inside = contains_form<F>(d, s, x, contain);
+      if (F == 4 && inside == pred::kUndecided) {
+        defer_contains(d, i, s);
+      } else if (inside) {
         hits.source[hits.count] = s;
         hits.depth[hits.count] = value(d.scores[s], x);
         ++hits.count;
@@ -698,7 +741,12 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
       double depth = 0.0;
       if ((batch >> lane) & 1u) {
         s = __ldg(&d.source_tree.ids[first + lane]);
-        hit = contains_flat<F>(d, s, x, contain);
+        const int inside = contains_form<F>(d, s, x, contain);
+        if (F == 4 && inside == pred::kUndecided) {
+          defer_contains(d, i, s);
+        } else {
+          hit = inside != 0;
+        }
         if (hit) depth = value(d.scores[s], x);
       }
       const unsigned hits = __ballot_sync(full, hit);
@@ -728,6 +776,29 @@ __global__ void __launch_bounds__(kBlock) k_heavy_hits(Dev d) {
   if constexpr (F == 2) contain.flush(d, kPredContain);
 }
 
+// The exact pass over the containment tests the filter-only ray kernels left
+// undecided: each hit joins its group's pool like the others (the group sort
+// orders a group's hits whatever their slots).
+__global__ void k_ray_exact(Dev d) {
+  if (d.status[kError] != 0) return;
+  const long long total = min(int64_t(d.sc[kRayDeferred]), d.ray_defer_cap);
+  if (tid() == 0) d.metrics[kDeferredContainTests] = d.sc[kRayDeferred];
+  Tally contain;
+  for (int64_t k = tid(); k < total; k += stride()) {
+    const int2 job = d.ray_defer[k];
+    const V2 x = d.samples[job.x];
+    if (!contains_flat<3>(d, job.y, x, contain)) continue;
+    const long long slot = static_cast<long long>(atomicAdd(
+        reinterpret_cast<unsigned long long *>(&d.metrics[kRayHits]), 1ull));
+    if (slot < d.cap.hits) {
+      d.hit_depth[slot] = value(d.scores[job.y], x);
+      d.hit_src[slot] = job.y;
+      d.hit_group[slot] = job.x;
+    }
+    atomicAdd(&d.group_counts[job.x], 1);
+  }
+}
+
 __global__ void k_check_hits(Dev d) {
   long long total = d.metrics[kRayHits];
   if (total > d.cap.hits) set_error(d.status, kErrHits);
@@ -740,7 +811,7 @@ __global__ void k_check_hits(Dev d) {
 // scene's depth complexity: up to kGroupSort hits are sorted by one thread in
 // place; if any group is larger, every hit goes through the global stable
 // radix passes instead (the order is the same either way).
-constexpr int kGroupSort = 64;
+constexpr int kGroupSort = 128;
 
 __global__ void k_group_sizes(Dev d) {
   const int live = live_polygons(d);
@@ -773,13 +844,18 @@ __global__ void k_hit_place(Dev d) {
 // difference of their sources' depth planes at the group's sample, equal
 // depths by source: the order the binary64 keys give wherever rounding does
 // not decide it.
+// With filtered binary64 predicates the filter-only form (F = 4) sorts every
+// group whose comparisons its filters decide and lists the others; form 3
+// then sorts the listed groups (`deferred_pass`).
 template <int F>
-__global__ void k_group_sort(Dev d) {
+__global__ void k_group_sort(Dev d, int deferred_pass) {
   // After a hit-pool overflow the groups' counts exceed the hits stored.
   if (d.sc[kSortHits] != 0 || d.status[kError] != 0) return;
-  const int live = live_polygons(d);
+  const int live = deferred_pass ? d.sc[kSortDeferred] : live_polygons(d);
+  if (deferred_pass && tid() == 0) d.metrics[kDeferredHitGroups] = live;
   Tally order;
-  for (int64_t g = tid(); g < live; g += stride()) {
+  for (int64_t t = tid(); t < live; t += stride()) {
+    const int64_t g = deferred_pass ? d.rank_defer[t] : t;
     const int k = d.group_counts[g];
     if (k < 2) continue;
     int *ids = d.hit_ids + d.group_offsets[g];
@@ -804,7 +880,8 @@ __global__ void k_group_sort(Dev d) {
     } else {
       const V2 x = d.samples[g];
       double depth[kGroupSort];
-      for (int j = 0; j < k; ++j) {
+      bool undecided = false;
+      for (int j = 0; j < k && !undecided; ++j) {
         const int h = ids[j];
         const double zj = d.hit_depth[h];
         const int sj = d.hit_src[h];
@@ -814,6 +891,10 @@ __global__ void k_group_sort(Dev d) {
           int stage = 0;
           const int o = order_sign<F>(d.scores[src[m]], depth[m], pj, zj, x, stage);
           if constexpr (F == 2) order.add(stage);
+          if (F == 4 && o == pred::kUndecided) {
+            undecided = true;
+            break;
+          }
           if (!(o > 0 || (o == 0 && src[m] > sj))) break;
           depth[m + 1] = depth[m];
           src[m + 1] = src[m];
@@ -823,6 +904,10 @@ __global__ void k_group_sort(Dev d) {
         depth[m + 1] = zj;
         src[m + 1] = sj;
         id[m + 1] = h;
+      }
+      if (undecided) {  // form 4: the exact pass sorts this group
+        d.rank_defer[atomicAdd(&d.sc[kSortDeferred], 1)] = int(g);
+        continue;
       }
     }
     for (int j = 0; j < k; ++j) ids[j] = id[j];
@@ -854,13 +939,18 @@ __global__ void k_hit_keys(Dev d, int stage) {
 // The filtered forms search with the exact order of k_group_sort when the
 // groups were sorted there, and with the binary64 order after the radix
 // passes (groups deeper than kGroupSort), matching the order searched.
+// With filtered binary64 predicates the filter-only form (F = 4) places every
+// polygon whose search its filters decide and lists the others; form 3 then
+// places the listed ones (`deferred_pass`).
 template <int F>
-__global__ void k_assign(Dev d) {
-  const int live = live_polygons(d);
+__global__ void k_assign(Dev d, int deferred_pass) {
+  const int live = deferred_pass ? d.sc[kAssignDeferred] : live_polygons(d);
+  if (deferred_pass && tid() == 0) d.metrics[kDeferredPolygons] = live;
   const bool exact = F != 0 && d.sc[kSortHits] == 0;
   Tally order;
-  for (int64_t i = tid(); i < live; i += stride()) {
+  for (int64_t t = tid(); t < live; t += stride()) {
     if (d.status[kError] != 0) return;
+    const int64_t i = deferred_pass ? d.rank_defer[t] : t;
     int source = d.out_src[d.reps[i]];
     V2 x = d.samples[i];
     const Plane ps = d.scores[source];
@@ -868,6 +958,7 @@ __global__ void k_assign(Dev d) {
     int g = d.groups[i];
     int low = 0, high = d.group_counts[g];
     const int *ids = d.hit_ids + d.group_offsets[g];
+    bool undecided = false;
     while (low < high) {
       int mid = (low + high) / 2;
       int h = ids[mid];
@@ -879,6 +970,10 @@ __global__ void k_assign(Dev d) {
         int stage = 0;
         const int o = order_sign<F>(ph, hz, ps, z, x, stage);
         if constexpr (F == 2) order.add(stage);
+        if (F == 4 && o == pred::kUndecided) {
+          undecided = true;
+          break;
+        }
         nearer = o < 0 || (o == 0 && hs < source);
       } else {
         nearer = hz < z || (hz == z && hs < source);
@@ -887,6 +982,10 @@ __global__ void k_assign(Dev d) {
         low = mid + 1;
       else
         high = mid;
+    }
+    if (undecided) {  // form 4: the exact pass places this polygon
+      d.rank_defer[atomicAdd(&d.sc[kAssignDeferred], 1)] = int(i);
+      continue;
     }
     d.out_layer[i] = low;
     if (low >= d.limit) {
@@ -1087,10 +1186,23 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
     note_launch();
   }
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_GRID, st));
-  EDP_LAUNCH_FORM(d.predicates, k_ray_hits, blocks(R), kBlock, st, d);
+  // Filtered binary64 predicates: the filter-only kernels, then exact passes
+  // over what their filters left undecided (same results as form 3 alone).
+  const bool split_exact = d.predicates == 3;
+  if (split_exact) {
+    k_ray_hits<4><<<blocks(R), kBlock, 0, st>>>(d);
+  } else {
+    EDP_LAUNCH_FORM(d.predicates, k_ray_hits, blocks(R), kBlock, st, d);
+  }
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_PRIMARY, st));
-  EDP_LAUNCH_FORM(d.predicates, k_heavy_hits, 148 * 16, kBlock, st, d);
+  if (split_exact) {
+    k_heavy_hits<4><<<148 * 16, kBlock, 0, st>>>(d);
+    note_launch();
+    k_ray_exact<<<148 * 4, kBlock, 0, st>>>(d);
+  } else {
+    EDP_LAUNCH_FORM(d.predicates, k_heavy_hits, 148 * 16, kBlock, st, d);
+  }
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_RAY_HEAVY, st));
   EDP_CHECK(scan_exclusive(d.group_counts, d.group_offsets, d.sc + kLivePolygons, R, nullptr, s, st));
@@ -1149,12 +1261,24 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   EDP_CHECK(cudaMemsetAsync(d.group_fill, 0, sizeof(int) * R, st));
   k_hit_place<<<blocks(d.cap.hits), kBlock, 0, st>>>(d);
   note_launch();
-  EDP_LAUNCH_FORM(d.predicates, k_group_sort, blocks(R), kBlock, st, d);
+  if (split_exact) {
+    k_group_sort<4><<<blocks(R), kBlock, 0, st>>>(d, 0);
+    note_launch();
+    k_group_sort<3><<<148 * 4, kBlock, 0, st>>>(d, 1);
+  } else {
+    EDP_LAUNCH_FORM(d.predicates, k_group_sort, blocks(R), kBlock, st, d, 0);
+  }
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_HIT_SORT, st));
   k_layers_reset<<<1, 1, 0, st>>>(d);
   note_launch();
-  EDP_LAUNCH_FORM(d.predicates, k_assign, blocks(R), kBlock, st, d);
+  if (split_exact) {
+    k_assign<4><<<blocks(R), kBlock, 0, st>>>(d, 0);
+    note_launch();
+    k_assign<3><<<148 * 4, kBlock, 0, st>>>(d, 1);
+  } else {
+    EDP_LAUNCH_FORM(d.predicates, k_assign, blocks(R), kBlock, st, d, 0);
+  }
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_ASSIGN, st));
   if (d.merge_regions) {

@@ -186,6 +186,7 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.seg_near, S));
   EDP_CHECK(alloc(p, &d.seg_near_src, S));
   EDP_CHECK(alloc(p, &d.seg_near_mag, S));
+  EDP_CHECK(alloc(p, &d.seg_vid, S));
   EDP_CHECK(alloc(p, &d.seg_lo, S));
   EDP_CHECK(alloc(p, &d.seg_hi, S));
   EDP_CHECK(alloc(p, &d.seg_slot, S));
@@ -229,6 +230,9 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.group_counts, R));
   EDP_CHECK(alloc(p, &d.group_offsets, R));
   EDP_CHECK(alloc(p, &d.group_fill, R));
+  EDP_CHECK(alloc(p, &d.rank_defer, R));
+  d.ray_defer_cap = H / 8 + 1024;
+  EDP_CHECK(alloc(p, &d.ray_defer, d.ray_defer_cap));
   EDP_CHECK(alloc(p, &d.tasks, E));
   EDP_CHECK(alloc(p, &d.owners, E));
   EDP_CHECK(alloc(p, &d.starts, E));

@@ -8,7 +8,7 @@ import ctypes
 from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libedp_b200.so"
-ABI_VERSION = 4  # EDP_ABI_VERSION in include/edp.h
+ABI_VERSION = 5  # EDP_ABI_VERSION in include/edp.h
 
 I64 = ctypes.c_int64
 I32 = ctypes.c_int32

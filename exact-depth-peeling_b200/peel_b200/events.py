@@ -39,7 +39,8 @@ METRIC_NAMES = (
     "ray_hits", "rounds", "unique_contours", "heavy_ray_groups", "beam_attempts",
     "certified_beams", "beam_candidate_tests", "heavy_beams", "rank_components",
     "rank_connections", "connection_contour_tests", "merged_polygons", "matched_patch_edges",
-    "edge_hash_misses", "heavy_noded_polygons",
+    "edge_hash_misses", "heavy_noded_polygons", "parked_patches", "deferred_contain_tests",
+    "deferred_hit_groups", "deferred_polygons",
 )
 assert len(METRIC_NAMES) == METRIC_COUNT
 

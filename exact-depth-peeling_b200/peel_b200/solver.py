@@ -12,7 +12,7 @@ import numpy as np
 
 from . import _lib
 
-METRIC_COUNT = 20  # EDP_METRICS: workspace counters (include/edp.h)
+METRIC_COUNT = 24  # EDP_METRICS: workspace counters (include/edp.h)
 
 _ERROR_LABELS = {
     1: "polygon vertices",

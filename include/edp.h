@@ -45,8 +45,8 @@ enum edp_status {
 /* Status slots and error bits (warp_peel/kernels.py:17-21, README.md:175-184). */
 enum {
   EDP_STATUS_SLOTS = 16,
-  EDP_METRICS = 20,
-  EDP_ABI_VERSION = 4,
+  EDP_METRICS = 24,
+  EDP_ABI_VERSION = 5,
   EDP_ERR_BIT_POLYGON = 1,
   EDP_ERR_BIT_WORKER = 2,
   EDP_ERR_BIT_RESIDUAL = 4,
@@ -128,7 +128,7 @@ int edp_enqueue(edp_peeler *p, void *stream);
 int edp_capture(edp_peeler *p);
 /* Asynchronous replay of the captured graph on the workspace stream. */
 int edp_run(edp_peeler *p);
-/* Synchronise the workspace stream and copy status[16] / metrics[20] out
+/* Synchronise the workspace stream and copy status[16] / metrics[24] out
  * (either may be NULL). */
 int edp_read_status(edp_peeler *p, int32_t *status, int64_t *metrics);
 int edp_get_outputs(edp_peeler *p, edp_outputs *out);
@@ -146,7 +146,11 @@ int edp_run_stage(edp_peeler *p, int32_t stage);
  * escalating filters (binary32 with a static error bound, then binary64, then
  * exact expansion arithmetic), optionally tallied per class and deciding
  * stage.  Workspaces start FILTERED64 (the faster exact form on a B200).
- * Constructions stay binary64. */
+ * Constructions stay binary64.  FILTERED64 runs each kernel with exact signs
+ * as two passes: binary64 filters alone, which leave what they cannot decide
+ * (a subdivision patch from the undecided test on, a containment test, a
+ * hit group, a polygon's rank search) to a second pass with the exact stage;
+ * metrics[20..23] count that work per extraction. */
 enum edp_predicates {
   EDP_PREDICATES_BINARY64 = 0,
   EDP_PREDICATES_FILTERED = 1,   /* binary32 filter, binary64 filter, exact */
@@ -288,8 +292,9 @@ const char *edp_status_string(int code);
 int edp_last_cuda_error(void);
 /* Source location ("file:line") of the CUDA call behind the last EDP_ERR_CUDA. */
 const char *edp_last_error_site(void);
-/* EDP_ABI_VERSION of the library: 4 since the predicate forms, 3 since
- * edp_stage_times; 2 had metrics[] of 20 counters (heavy_noded_polygons
+/* EDP_ABI_VERSION of the library: 5 since metrics[] has 24 counters (the
+ * filtered binary64 form's deferred work); 4 since the predicate forms, 3
+ * since edp_stage_times; 2 had metrics[] of 20 counters (heavy_noded_polygons
  * added); 1 had 19. */
 int edp_abi_version(void);
 

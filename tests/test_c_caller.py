@@ -26,4 +26,4 @@ def test_c_program_links_and_calls(tmp_path):
                     f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)], check=True)
     done = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert done.returncode == 0, done.stderr
-    assert done.stdout.split() == ["abi", "4", "metrics", "20", "status", "16"]
+    assert done.stdout.split() == ["abi", "5", "metrics", "24", "status", "16"]

@@ -29,6 +29,8 @@ def lib(tmp_path_factory):
     handle.orient2d_batch.argtypes = [P, ctypes.c_long, P, P]
     handle.orient2d_lean_batch.argtypes = [P, ctypes.c_long, P, P]
     handle.dot_sign_batch.argtypes = [P, P, ctypes.c_int, ctypes.c_long, P, P]
+    handle.orient2d_filter_batch.argtypes = [P, ctypes.c_long, P]
+    handle.dot_sign_filter_batch.argtypes = [P, P, ctypes.c_int, ctypes.c_long, P]
     return handle
 
 
@@ -178,3 +180,39 @@ def test_lean_filter_gives_the_same_signs(lib):
     stages = np.zeros(2, dtype=np.int32)
     lib.orient2d_lean_batch(grid.ctypes.data, 2, signs.ctypes.data, stages.ctypes.data)
     assert signs.tolist() == [0, 0]
+
+
+UNDECIDED = 2
+
+
+def test_filter_only_stages_decide_or_defer(lib):
+    """The first pass of the two-pass form (orient2d_filter, dot_sign_filter)
+    gives the exact sign wherever it decides and kUndecided otherwise; it
+    defers exactly where orient2d_lean and dot_sign reach their exact stage."""
+    rng = np.random.default_rng(8)
+    a = rng.uniform(-1, 1, size=(400, 2))
+    b = rng.uniform(-1, 1, size=(400, 2))
+    on_line = a + rng.uniform(-2, 2, size=(400, 1)) * (b - a)
+    near = on_line + rng.normal(scale=1e-15, size=on_line.shape)
+    for c in (rng.uniform(-1, 1, size=(400, 2)), on_line, near):
+        rows = np.ascontiguousarray(np.hstack([a, b, c]), dtype=np.float64)
+        got = np.zeros(len(rows), dtype=np.int32)
+        lib.orient2d_filter_batch(rows.ctypes.data, len(rows), got.ctypes.data)
+        lean = np.zeros(len(rows), dtype=np.int32)
+        stages = np.zeros(len(rows), dtype=np.int32)
+        lib.orient2d_lean_batch(rows.ctypes.data, len(rows), lean.ctypes.data,
+                                stages.ctypes.data)
+        np.testing.assert_array_equal(got == UNDECIDED, stages == EXACT)
+        decided = got != UNDECIDED
+        np.testing.assert_array_equal(got[decided], lean[decided])
+    p = rng.normal(size=(300, 6))
+    q = rng.normal(size=(300, 6))
+    q[:150, -1] = -(p[:150, :-1] * q[:150, :-1]).sum(axis=1) / p[:150, -1]
+    p, q = np.ascontiguousarray(p), np.ascontiguousarray(q)
+    got = np.zeros(len(p), dtype=np.int32)
+    lib.dot_sign_filter_batch(p.ctypes.data, q.ctypes.data, 6, len(p), got.ctypes.data)
+    signs, stages = dots(lib, p, q)
+    np.testing.assert_array_equal(got == UNDECIDED, stages == EXACT)
+    decided = got != UNDECIDED
+    np.testing.assert_array_equal(got[decided], signs[decided])
+    assert (~decided).any() and decided.any()
