@@ -67,9 +67,18 @@ struct Tally {
 
 __device__ inline int sign_of(double v) { return (v > 0.0) - (v < 0.0); }
 
-// Side of c against the line a->b: +1 left, -1 right, 0 on it.
+// Side of c against the line a->b: +1 left, -1 right, 0 on it.  In the
+// filtered forms a point equal to an end of the line is on it without
+// arithmetic (the filters cannot certify a zero; shared mesh vertices make
+// this case common); it is counted with the binary64 stage.
 template <int F>
 __device__ inline int side_sign(V2 a, V2 b, V2 c, int &stage) {
+  if constexpr (F != 0) {
+    if ((c.x == a.x && c.y == a.y) || (c.x == b.x && c.y == b.y)) {
+      stage = pred::kBinary64;
+      return 0;
+    }
+  }
   if constexpr (F == 0) {
     return sign_of(cross(a, b, c));
   } else if constexpr (F == 3) {

@@ -209,8 +209,11 @@ OVERFLOW = 2 | 4 | 8 | 16 | 32 | 64 | 1024 | 2048  # pool-capacity bits of statu
 
 def peel(arrays, sizer=None, scale=1.0, **options):
     """Extract with learned pools; on a pool overflow, extract again with the
-    conservative ``EventCapacities.for_mesh`` pools.  Returns (peeler,
-    capacities, fell_back)."""
+    conservative ``EventCapacities.for_mesh`` pools, doubled where even they
+    overflow (``sizing.fit_event_capacities``).  Returns (peeler, capacities,
+    fell_back)."""
+    from .sizing import fit_event_capacities
+
     sizer = sizer or PoolSizer(device=arrays[0].device)
     cap = sizer.capacities(arrays, scale)
     p = EventPeeler(*arrays, capacities=cap, **options)
@@ -218,9 +221,8 @@ def peel(arrays, sizer=None, scale=1.0, **options):
     p.stream.synchronize()
     if int(p.status[9].item()) & OVERFLOW:
         del p
-        cap = EventCapacities.for_mesh(arrays[1].shape[0])
-        p = EventPeeler(*arrays, capacities=cap, **options)
-        p.run()
+        p, cap = fit_event_capacities(arrays, EventCapacities.for_mesh(arrays[1].shape[0]),
+                                      headroom=1.0, **options)
         return p, cap, True
     return p, cap, False
 
