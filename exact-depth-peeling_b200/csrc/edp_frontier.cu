@@ -548,7 +548,9 @@ cudaError_t stage_step(const Dev &d, cudaStream_t st) {
   if (d.predicates == 3) {  // filtered binary64: filter-only pass, then the exact pass
     k_subdivide<4><<<unsigned(g), kBlock, 0, st>>>(d, 0);
     note_launch();
-    k_subdivide<3><<<unsigned(g), kBlock, 0, st>>>(d, 1);
+    // Few patches are parked (a few thousand per extraction on the knot): a
+    // small grid takes them from the counter.
+    k_subdivide<3><<<unsigned(g < 296 ? g : 296), kBlock, 0, st>>>(d, 1);
   } else {
     EDP_LAUNCH_FORM(d.predicates, k_subdivide, unsigned(g), kBlock, st, d, 0);
   }

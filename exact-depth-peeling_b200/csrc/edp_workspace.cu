@@ -764,7 +764,9 @@ int edp_stage_times(edp_peeler *p, float *ms) {
 
 int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round) {
   if (!p || !outside_loop || !per_round) return EDP_ERR_ARGUMENT;
-  if (!p->exec) return EDP_ERR_STATE;
+  // Counted whenever the extraction was recorded into a graph: the
+  // workspace's own (edp_capture) or a caller's (edp_enqueue).
+  if (!p->exec && p->kernels_outside == 0) return EDP_ERR_STATE;
   *outside_loop = p->kernels_outside;
   *per_round = p->kernels_per_round;
   return EDP_OK;

@@ -227,8 +227,10 @@ enum edp_stage {
  * reference, whose profiler captures each stage as a separate graph. */
 int edp_stage_times(edp_peeler *p, float *ms);
 
-/* Kernel nodes of the captured graph: outside the subdivision loop, and per
- * loop iteration (a replay launches outside + per_round * rounds kernels). */
+/* Kernel nodes of the captured graph (the workspace's own, or the caller's
+ * graph that edp_enqueue recorded it into): outside the subdivision loop, and
+ * per loop iteration (a replay launches outside + per_round * rounds
+ * kernels). */
 int edp_graph_kernels(edp_peeler *p, int64_t *outside_loop, int64_t *per_round);
 
 /* Exact-position welding without any device allocation.  No counterpart in the
