@@ -105,18 +105,15 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
   const int lane = threadIdx.x & 31;
   const bool mine = lane < n;
   const int width = lane_width(n);
-  V2 ca = v2(0.0, 0.0), cb = ca, cn = ca, cm = ca;
-  int2 cs = make_int2(0, 0), cv = make_int2(-1, -1);
+  V2 ca = v2(0.0, 0.0), cb = ca, cn = ca;
+  int cid = 0;  // the lane's candidate: its near sources and vertices are read only
+                // where a depth filter leaves the sign open (rare)
   if ((batch >> lane) & 1u) {
     const int c = __ldg(&g.ids[first + lane]);
+    cid = c;
     ca = g.a[c];
     cb = g.b[c];
     cn = g.near[c];
-    if constexpr (F != 0) {
-      cs = g.near_src[c];
-      cm = g.near_mag[c];
-      cv = g.vid[c];
-    }
   }
   while (batch) {
     const int k = __ffs(int(batch)) - 1;
@@ -152,30 +149,35 @@ __device__ inline int first_cut(Segments g, unsigned batch, int first, V2 p, V2 
       // two planes compared exactly (zero when the source is the patch's
       // own).
       int stage_b = 0;
-      const V2 mag = shfl(cm, k);
+      const V2 mag = g.near_mag[__shfl_sync(kFull, cid, k)];
       const double bound_a = 4.0 * pred::kU64 *
           (fabs(sc.a * a.x) + fabs(sc.b * a.y) + fabs(sc.c) + mag.x);
       const double bound_b = 4.0 * pred::kU64 *
           (fabs(sc.a * b.x) + fabs(sc.b * b.y) + fabs(sc.c) + mag.y);
-      const int sa = __shfl_sync(kFull, cs.x, k), sb = __shfl_sync(kFull, cs.y, k);
-      const int va = __shfl_sync(kFull, cv.x, k), vb = __shfl_sync(kFull, cv.y, k);
+      const int c = __shfl_sync(kFull, cid, k);
       if (fabs(za) > bound_a) {
         sza = sign_of(za);
         stage = pred::kBinary64;
-      } else if (has_vertex(g, source, va) && has_vertex(g, sa, va)) {
-        sza = 0;
-        stage = pred::kBinary64;
       } else {
-        sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
+        const int sa = g.near_src[c].x, va = g.vid[c].x;
+        if (has_vertex(g, source, va) && has_vertex(g, sa, va)) {
+          sza = 0;
+          stage = pred::kBinary64;
+        } else {
+          sza = order_sign<F>(sc, value(sc, a), g.scores[sa], near.x, a, stage);
+        }
       }
       if (fabs(zb) > bound_b) {
         szb = sign_of(zb);
         stage_b = pred::kBinary64;
-      } else if (has_vertex(g, source, vb) && has_vertex(g, sb, vb)) {
-        szb = 0;
-        stage_b = pred::kBinary64;
       } else {
-        szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
+        const int sb = g.near_src[c].y, vb = g.vid[c].y;
+        if (has_vertex(g, source, vb) && has_vertex(g, sb, vb)) {
+          szb = 0;
+          stage_b = pred::kBinary64;
+        } else {
+          szb = order_sign<F>(sc, value(sc, b), g.scores[sb], near.y, b, stage_b);
+        }
       }
       if constexpr (F == 2) {
         if (lane == 0) {  // the same test on every lane: count it once
