@@ -134,6 +134,7 @@ enum Scalar : int {
   kRayDeferred = 28,
   kSortDeferred = 29,
   kAssignDeferred = 30,
+  kDeepGroups = 31,  // hit groups sorted a warp each (k_group_sort_deep)
   kScalarCount = 32  // k_reset clears them with one warp
 };
 
@@ -227,6 +228,7 @@ struct Dev {
   int2 *ray_defer;
   int64_t ray_defer_cap;
   int *rank_defer;  // [regions]
+  int *deep_groups; // [regions]: hit groups too deep for one thread's sort
   // Optional convex merging: each polygon's chosen patch edge, and the
   // compaction copy of the outputs (allocated with merge_regions only).
   int *merge_choice;

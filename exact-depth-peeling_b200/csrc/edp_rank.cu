@@ -812,6 +812,9 @@ __global__ void k_check_hits(Dev d) {
 // place; if any group is larger, every hit goes through the global stable
 // radix passes instead (the order is the same either way).
 constexpr int kGroupSort = 128;
+// Groups deeper than this are sorted a warp each (k_group_sort_deep): one
+// thread's insertion sort of a deep group held its warp's other lanes.
+constexpr int kWarpSort = 32;
 
 __global__ void k_group_sizes(Dev d) {
   const int live = live_polygons(d);
@@ -858,6 +861,10 @@ __global__ void k_group_sort(Dev d, int deferred_pass) {
     const int64_t g = deferred_pass ? d.rank_defer[t] : t;
     const int k = d.group_counts[g];
     if (k < 2) continue;
+    if (!deferred_pass && k > kWarpSort) {  // sorted a warp each by k_group_sort_deep
+      d.deep_groups[atomicAdd(&d.sc[kDeepGroups], 1)] = int(g);
+      continue;
+    }
     int *ids = d.hit_ids + d.group_offsets[g];
     int src[kGroupSort], id[kGroupSort];
     if constexpr (F == 0) {
@@ -930,6 +937,102 @@ __global__ void k_group_sort(Dev d, int deferred_pass) {
       }
     }
     for (int j = 0; j < k; ++j) ids[j] = id[j];
+  }
+  if constexpr (F == 2) order.flush(d, kPredOrder);
+}
+
+// The groups of more than kWarpSort (and at most kGroupSort) hits, a warp
+// each.  The group's hits and their sources' planes go to shared memory; each
+// lane counts, for each of its hits, the hits whose (ordered binary64 depth
+// bits, source) key comes first, which is the hit's place in key order (the
+// keys are distinct: one hit per source).  That is the plain form's order.
+// The filtered forms order by the exact sign of the plane difference at the
+// group's sample, then by source; they check the key order's neighbours with
+// that comparison (a total order is sorted when its neighbours are), and a
+// group that fails the check, or meets an undecided filter (F = 4), is sorted
+// by insertion on lane 0 (forms 1-3) or goes to the exact pass's list (4).
+template <int F>
+__global__ void __launch_bounds__(kBlock) k_group_sort_deep(Dev d) {
+  if (d.sc[kSortHits] != 0 || d.status[kError] != 0) return;
+  constexpr int kWarpsPerBlock = kBlock / 32;
+  __shared__ double s_depth[kWarpsPerBlock][kGroupSort];
+  __shared__ Plane s_plane[kWarpsPerBlock][kGroupSort];
+  __shared__ int s_src[kWarpsPerBlock][kGroupSort], s_id[kWarpsPerBlock][kGroupSort];
+  __shared__ unsigned char s_order[kWarpsPerBlock][kGroupSort];  // key order -> hit
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int deep = d.sc[kDeepGroups];
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  Tally order;
+  for (int64_t t = tid() >> 5; t < deep; t += warps) {
+    const int g = d.deep_groups[t];
+    const int k = d.group_counts[g];
+    int *ids = d.hit_ids + d.group_offsets[g];
+    for (int j = lane; j < k; j += 32) {
+      const int h = ids[j];
+      s_depth[w][j] = d.hit_depth[h];
+      s_src[w][j] = d.hit_src[h];
+      if constexpr (F != 0) s_plane[w][j] = d.scores[s_src[w][j]];
+      s_id[w][j] = h;
+    }
+    __syncwarp();
+    for (int j = lane; j < k; j += 32) {
+      const unsigned long long kj = ordered_bits(s_depth[w][j]);
+      const int sj = s_src[w][j];
+      int before = 0;
+      for (int i = 0; i < k; ++i) {
+        const unsigned long long ki = ordered_bits(s_depth[w][i]);
+        before += ki < kj || (ki == kj && s_src[w][i] < sj);
+      }
+      s_order[w][before] = (unsigned char)j;
+    }
+    __syncwarp();
+    bool sorted = true, undecided = false;
+    if constexpr (F != 0) {
+      const V2 x = d.samples[g];
+      for (int m = lane; m + 1 < k; m += 32) {
+        const int a = s_order[w][m], b = s_order[w][m + 1];
+        int stage = 0;
+        const int o = order_sign<F>(s_plane[w][a], s_depth[w][a], s_plane[w][b], s_depth[w][b],
+                                    x, stage);
+        if constexpr (F == 2) order.add(stage);
+        if (F == 4 && o == pred::kUndecided)
+          undecided = true;
+        else if (!(o < 0 || (o == 0 && s_src[w][a] < s_src[w][b])))
+          sorted = false;
+      }
+      undecided = __any_sync(0xffffffffu, undecided);
+      sorted = __all_sync(0xffffffffu, sorted);
+    }
+    if constexpr (F == 4) {
+      if (undecided || !sorted) {  // the exact pass sorts this group
+        if (lane == 0) d.rank_defer[atomicAdd(&d.sc[kSortDeferred], 1)] = g;
+        __syncwarp();
+        continue;
+      }
+    } else if constexpr (F != 0) {
+      if (!sorted && lane == 0) {  // rare: lane 0 sorts the key order exactly
+        const V2 x = d.samples[g];
+        unsigned char *o = s_order[w];
+        for (int j = 1; j < k; ++j) {
+          const int b = o[j];
+          int m = j - 1;
+          while (m >= 0) {
+            const int a = o[m];
+            int stage = 0;
+            const int c = order_sign<F>(s_plane[w][a], s_depth[w][a], s_plane[w][b],
+                                        s_depth[w][b], x, stage);
+            if constexpr (F == 2) order.add(stage);
+            if (!(c > 0 || (c == 0 && s_src[w][a] > s_src[w][b]))) break;
+            o[m + 1] = o[m];
+            --m;
+          }
+          o[m + 1] = (unsigned char)b;
+        }
+      }
+      __syncwarp();
+    }
+    for (int m = lane; m < k; m += 32) ids[m] = s_id[w][s_order[w][m]];
+    __syncwarp();
   }
   if constexpr (F == 2) order.flush(d, kPredOrder);
 }
@@ -1283,9 +1386,13 @@ cudaError_t stage_rank(const Dev &d, SortScratch &s, cudaStream_t st) {
   if (split_exact) {
     k_group_sort<4><<<blocks(R), kBlock, 0, st>>>(d, 0);
     note_launch();
+    k_group_sort_deep<4><<<148 * 8, kBlock, 0, st>>>(d);
+    note_launch();
     k_group_sort<3><<<148 * 4, kBlock, 0, st>>>(d, 1);
   } else {
     EDP_LAUNCH_FORM(d.predicates, k_group_sort, blocks(R), kBlock, st, d, 0);
+    note_launch();
+    EDP_LAUNCH_FORM(d.predicates, k_group_sort_deep, 148 * 8, kBlock, st, d);
   }
   note_launch();
   EDP_CHECK(stage_mark(EDP_STAGE_RANK_HIT_SORT, st));

@@ -231,6 +231,7 @@ cudaError_t allocate_event(edp_peeler *p) {
   EDP_CHECK(alloc(p, &d.group_offsets, R));
   EDP_CHECK(alloc(p, &d.group_fill, R));
   EDP_CHECK(alloc(p, &d.rank_defer, R));
+  EDP_CHECK(alloc(p, &d.deep_groups, R));
   d.ray_defer_cap = H / 8 + 1024;
   EDP_CHECK(alloc(p, &d.ray_defer, d.ray_defer_cap));
   EDP_CHECK(alloc(p, &d.tasks, E));
