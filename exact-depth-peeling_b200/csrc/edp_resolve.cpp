@@ -285,8 +285,22 @@ void shr1_in_place(Int &r) {
   r.set_size(r.size(), false);
 }
 
+// The leading 64 bits of |a| (a != 0) as m 2^e, m in [2^63, 2^64), truncated:
+// |a| = m 2^e (1 + t) with 0 <= t < 2^-63.
+long double leading(const Int &a, int &e) {
+  const int n = a.size(), top = a.bits() - 64 * (n - 1);  // bits in the top limb
+  const u64 hi = a.limbs()[n - 1];
+  u64 m = top == 64 ? hi : (hi << (64 - top)) | (n > 1 ? a.limbs()[n - 2] >> top : 0);
+  e = a.bits() - 64;
+  return static_cast<long double>(m);
+}
+
 // Correctly rounded binary64 value of num / (den * 2^scale), den > 0 (round
 // to nearest, ties to even); results outside the normal range are refused.
+// Most values are settled by the leading bits: the quotient of the truncated
+// leading 64 bits (x87 extended precision) is within 2^-61 of the exact
+// value, and when both ends of that interval round to the same binary64 value
+// it is the answer; otherwise binary long division decides.
 double to_double(const Int &num, const Int &den, int scale) {
   if (num.sign() == 0) return 0.0;
   if (den.size() == 1 && den.limbs()[0] == 1 && num.bits() <= 53) {
@@ -294,6 +308,15 @@ double to_double(const Int &num, const Int &den, int scale) {
     const double v = std::ldexp(double(num.limbs()[0]), -scale);
     if (!(v >= 0x1p-1022) || !std::isfinite(v)) throw TooLarge{};
     return num.negative() ? -v : v;
+  }
+  {
+    int en, ed;
+    const long double mn = leading(num, en), md = leading(den, ed);
+    const long double q = std::ldexp(mn / md, en - ed - scale);
+    const long double eps = 0x1p-60L;
+    const double lo = static_cast<double>(q * (1.0L - eps));
+    const double hi = static_cast<double>(q * (1.0L + eps));
+    if (lo == hi && std::isfinite(lo) && lo >= 0x1p-1022) return num.negative() ? -lo : lo;
   }
   Int a = num;
   if (a.negative()) a.negate();
